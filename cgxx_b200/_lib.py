@@ -1,0 +1,294 @@
+"""ctypes binding of libcgb200.so (the C ABI declared in include/cgx.h).
+
+The library is built in-tree by cgxx_b200.build; loading fails loudly if it
+is missing -- there is no CPU fallback.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libcgb200.so")
+
+SUCCESS = 0
+STATUS_NAMES = {
+    0: "SUCCESS", 1: "INVALID_ARGUMENT", 2: "INVALID_STATE", 3: "UNSUPPORTED",
+    4: "CUDA", 5: "OUT_OF_MEMORY", 6: "DEVICE", 7: "IO", 8: "NUMERICAL",
+}
+
+# cgx_vector (CG::Vector order, CG.h:22-35)
+VECTOR_K, VECTOR_X, VECTOR_P, VECTOR_Q, VECTOR_R, VECTOR_Z = range(6)
+VECTORS = {"K": 0, "X": 1, "P": 2, "Q": 3, "R": 4, "Z": 5}
+# cgx_format (CG::MatrixFormat order, CG.h:38-47)
+FORMAT_COO, FORMAT_CRS, FORMAT_ELL = range(3)
+PRECOND_NONE, PRECOND_JACOBI, PRECOND_LEARNED = range(3)
+PRECISION_FP64, PRECISION_MIXED = range(2)
+LOOP_GRAPH, LOOP_CHUNKED, LOOP_KERNELS = range(3)
+
+
+class Options(C.Structure):
+    _fields_ = [
+        ("max_iterations", C.c_int),
+        ("tolerance", C.c_double),
+        ("preconditioner", C.c_int),
+        ("precision", C.c_int),
+        ("loop", C.c_int),
+        ("inner_tolerance", C.c_double),
+        ("max_outer", C.c_int),
+        ("compute_true_residual", C.c_int),
+    ]
+
+
+class Result(C.Structure):
+    _fields_ = [
+        ("iterations", C.c_int),
+        ("residual", C.c_double),
+        ("true_residual", C.c_double),
+        ("converged", C.c_int),
+        ("outer_iterations", C.c_int),
+        ("solve_ms", C.c_double),
+        ("spmv_ms", C.c_double),
+        ("update_ms", C.c_double),
+        ("direction_ms", C.c_double),
+        ("spmv_launches", C.c_int),
+        ("update_launches", C.c_int),
+        ("direction_launches", C.c_int),
+        ("fell_back", C.c_int),
+    ]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class CgxError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+        self.message = message
+
+
+_P = C.c_void_p
+_I = C.c_int
+_D = C.c_double
+_PI = C.POINTER(C.c_int)
+_PD = C.POINTER(C.c_double)
+
+# name -> argtypes (restype is the int status unless listed in _RESTYPE)
+PROTOTYPES = {
+    "cgx_version": [_PI, _PI],
+    "cgx_status_string": [_I],
+    "cgx_last_error": [],
+    "cgx_device_count": [_PI],
+    "cgx_default_options": [C.POINTER(Options)],
+    "cgx_create": [C.POINTER(_P), _I],
+    "cgx_destroy": [_P],
+    "cgx_set_stream": [_P, _P],
+    "cgx_synchronize": [_P],
+    "cgx_upload_crs": [_P, _I, _I, _P, _P, _P],
+    "cgx_upload_ell": [_P, _I, _I, _I, _P, _P, _P],
+    "cgx_upload_coo": [_P, _I, _I, _P, _P, _P],
+    "cgx_upload_jacobi": [_P, _P],
+    "cgx_jacobi_from_matrix": [_P],
+    "cgx_set_vector": [_P, _I, _P],
+    "cgx_get_vector": [_P, _I, _P],
+    "cgx_fill_vector": [_P, _I, _D],
+    "cgx_matrix_info": [_P, _PI, _PI, _PI],
+    "cgx_copy": [_P, _I, _I],
+    "cgx_matvec": [_P, _I, _I],
+    "cgx_axpy": [_P, _D, _I, _I],
+    "cgx_xpay": [_P, _I, _D, _I],
+    "cgx_dot": [_P, _I, _I, _PD],
+    "cgx_apply_jacobi": [_P, _I, _I],
+    "cgx_solve": [_P, C.POINTER(Options), C.POINTER(Result)],
+    "cgx_true_residual": [_P, _PD],
+    "cgx_mtx_read": [C.c_char_p, _PI, _PI, C.POINTER(_PI), C.POINTER(_PI),
+                     C.POINTER(_PD)],
+    "cgx_mtx_write_symmetric_crs": [C.c_char_p, _I, _P, _P, _P],
+    "cgx_free": [_P],
+}
+_RESTYPE = {"cgx_version": None, "cgx_status_string": C.c_char_p,
+            "cgx_last_error": C.c_char_p, "cgx_free": None}
+
+_lib = None
+
+
+def load():
+    """Loads libcgb200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is missing: build it with `python -m cgxx_b200.build`")
+        lib = C.CDLL(LIB_PATH)
+        for name, args in PROTOTYPES.items():
+            fn = getattr(lib, name)
+            fn.argtypes = args
+            fn.restype = _RESTYPE.get(name, C.c_int)
+        _lib = lib
+    return _lib
+
+
+def check(status):
+    if status != SUCCESS:
+        msg = load().cgx_last_error().decode(errors="replace")
+        raise CgxError(status, msg)
+
+
+def device_count():
+    n = C.c_int(0)
+    check(load().cgx_device_count(C.byref(n)))
+    return n.value
+
+
+def _arr(a, dtype):
+    a = np.ascontiguousarray(a, dtype=dtype)
+    return a, a.ctypes.data_as(C.c_void_p)
+
+
+def default_options(**kw):
+    o = Options()
+    check(load().cgx_default_options(C.byref(o)))
+    for k, v in kw.items():
+        if not hasattr(o, k):
+            raise KeyError(k)
+        setattr(o, k, v)
+    return o
+
+
+class Handle:
+    """One device-resident problem: matrix, Jacobi C and the vectors K..Z."""
+
+    def __init__(self, device=0):
+        self._lib = load()
+        self._h = C.c_void_p()
+        check(self._lib.cgx_create(C.byref(self._h), device))
+        self.N = 0
+
+    def close(self):
+        if self._h:
+            check(self._lib.cgx_destroy(self._h))
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # --- uploads (CGCUDA::doTransferTo) ---
+    def upload_crs(self, ptr, index, value):
+        ptr, pp = _arr(ptr, np.int32)
+        index, pi = _arr(index, np.int32)
+        value, pv = _arr(value, np.float64)
+        N = len(ptr) - 1
+        check(self._lib.cgx_upload_crs(self._h, N, len(index), pp, pi, pv))
+        self.N = N
+
+    def upload_ell(self, N, nz, max_nz, length, index, data):
+        length, pl = _arr(length, np.int32)
+        index, pi = _arr(index, np.int32)
+        data, pd = _arr(data, np.float64)
+        check(self._lib.cgx_upload_ell(self._h, N, nz, max_nz, pl, pi, pd))
+        self.N = N
+
+    def upload_coo(self, N, I, J, V):
+        I, pI = _arr(I, np.int32)
+        J, pJ = _arr(J, np.int32)
+        V, pV = _arr(V, np.float64)
+        check(self._lib.cgx_upload_coo(self._h, N, len(I), pI, pJ, pV))
+        self.N = N
+
+    def upload_jacobi(self, Cdiag):
+        Cdiag, pc = _arr(Cdiag, np.float64)
+        check(self._lib.cgx_upload_jacobi(self._h, pc))
+
+    def jacobi_from_matrix(self):
+        check(self._lib.cgx_jacobi_from_matrix(self._h))
+
+    # --- vectors ---
+    def set_vector(self, v, host):
+        host, p = _arr(host, np.float64)
+        assert host.size == self.N
+        check(self._lib.cgx_set_vector(self._h, VECTORS.get(v, v), p))
+
+    def get_vector(self, v):
+        out = np.empty(self.N, dtype=np.float64)
+        check(self._lib.cgx_get_vector(self._h, VECTORS.get(v, v),
+                                       out.ctypes.data_as(C.c_void_p)))
+        return out
+
+    def fill_vector(self, v, value):
+        check(self._lib.cgx_fill_vector(self._h, VECTORS.get(v, v), float(value)))
+
+    # --- per-kernel interface (CG.h:224-237) ---
+    def copy(self, dst, src):
+        check(self._lib.cgx_copy(self._h, VECTORS.get(dst, dst), VECTORS.get(src, src)))
+
+    def matvec(self, x, y):
+        check(self._lib.cgx_matvec(self._h, VECTORS.get(x, x), VECTORS.get(y, y)))
+
+    def axpy(self, a, x, y):
+        check(self._lib.cgx_axpy(self._h, float(a), VECTORS.get(x, x), VECTORS.get(y, y)))
+
+    def xpay(self, x, a, y):
+        check(self._lib.cgx_xpay(self._h, VECTORS.get(x, x), float(a), VECTORS.get(y, y)))
+
+    def dot(self, a, b):
+        r = C.c_double()
+        check(self._lib.cgx_dot(self._h, VECTORS.get(a, a), VECTORS.get(b, b), C.byref(r)))
+        return r.value
+
+    def apply_jacobi(self, x, y):
+        check(self._lib.cgx_apply_jacobi(self._h, VECTORS.get(x, x), VECTORS.get(y, y)))
+
+    def synchronize(self):
+        check(self._lib.cgx_synchronize(self._h))
+
+    # --- solve (CG::solve) ---
+    def solve(self, options=None, **kw):
+        o = options if options is not None else default_options(**kw)
+        r = Result()
+        check(self._lib.cgx_solve(self._h, C.byref(o), C.byref(r)))
+        return r.as_dict()
+
+    def true_residual(self):
+        r = C.c_double()
+        check(self._lib.cgx_true_residual(self._h, C.byref(r)))
+        return r.value
+
+
+def mtx_read(path):
+    """MatrixMarket reader with the reference's entry order (Matrix.cpp:13-111).
+    Returns (N, I, J, V) as numpy arrays."""
+    lib = load()
+    N = C.c_int()
+    nz = C.c_int()
+    I = _PI()
+    J = _PI()
+    V = _PD()
+    check(lib.cgx_mtx_read(os.fsencode(path), C.byref(N), C.byref(nz),
+                           C.byref(I), C.byref(J), C.byref(V)))
+    try:
+        n = nz.value
+        Ia = np.ctypeslib.as_array(I, shape=(n,)).copy() if n else np.zeros(0, np.int32)
+        Ja = np.ctypeslib.as_array(J, shape=(n,)).copy() if n else np.zeros(0, np.int32)
+        Va = np.ctypeslib.as_array(V, shape=(n,)).copy() if n else np.zeros(0, np.float64)
+    finally:
+        lib.cgx_free(C.cast(I, C.c_void_p))
+        lib.cgx_free(C.cast(J, C.c_void_p))
+        lib.cgx_free(C.cast(V, C.c_void_p))
+    return N.value, Ia, Ja, Va
+
+
+def mtx_write_symmetric_crs(path, ptr, index, value):
+    ptr, pp = _arr(ptr, np.int32)
+    index, pi = _arr(index, np.int32)
+    value, pv = _arr(value, np.float64)
+    check(load().cgx_mtx_write_symmetric_crs(os.fsencode(path), len(ptr) - 1, pp, pi, pv))

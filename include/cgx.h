@@ -1,0 +1,203 @@
+/*
+ * cgx.h -- C ABI of libcgb200, the B200 (sm_100a) conjugate-gradient engine.
+ *
+ * The reference (hahnjo/CGxx) plugs a programming model into its solver by
+ * deriving from the abstract class CG (CG.h:19-293) and overriding its
+ * per-kernel virtual methods (CG.h:180-237); the CUDA plug-in is
+ * cuda/CGCUDA.cu. Every entry point below names the reference method it
+ * replaces. A plug-in that binds this library needs nothing but these plain C
+ * declarations: no CUDA, torch or C++ types cross the boundary.
+ *
+ * Conventions
+ *   - Every function returns a cgx_status; CGX_SUCCESS is 0. On failure
+ *     cgx_last_error() returns a message for the calling thread. (The
+ *     reference instead prints "CUDA error: ..." and calls exit(1),
+ *     cuda/utils.h:10-15; the host CG class of this project converts a
+ *     failed status into exactly that behaviour.)
+ *   - Host pointers are ordinary (pageable or pinned) host memory; the
+ *     library copies from/to them. Pinned buffers make the copies faster.
+ *   - A handle is bound to one device and one CUDA stream and must be used by
+ *     one host thread at a time, like the reference's single-threaded CG.
+ *   - Matrices use 0-based int32 indices and double values, laid out exactly
+ *     as the reference's MatrixCRS / MatrixELL / MatrixCOO (Matrix.h:22-103).
+ */
+#ifndef CGX_H
+#define CGX_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CGX_VERSION_MAJOR 1
+#define CGX_VERSION_MINOR 0
+
+typedef struct cgx_handle cgx_handle;
+
+typedef enum cgx_status {
+  CGX_SUCCESS = 0,
+  CGX_ERROR_INVALID_ARGUMENT = 1, /* bad pointer, size, enum or matrix data */
+  CGX_ERROR_INVALID_STATE = 2,    /* e.g. solve before a matrix is uploaded */
+  CGX_ERROR_UNSUPPORTED = 3,      /* format/preconditioner/precision combo */
+  CGX_ERROR_CUDA = 4,             /* a CUDA runtime call failed */
+  CGX_ERROR_OUT_OF_MEMORY = 5,    /* device allocation failed */
+  CGX_ERROR_DEVICE = 6,           /* a device-side check failed (see text) */
+  CGX_ERROR_IO = 7,               /* MatrixMarket file could not be read */
+  CGX_ERROR_NUMERICAL = 8         /* NaN/Inf or breakdown that ended a solve */
+} cgx_status;
+
+/* CG::Vector (CG.h:22-35), same order and meaning. */
+typedef enum cgx_vector {
+  CGX_VECTOR_K = 0, /* right-hand side */
+  CGX_VECTOR_X = 1, /* solution */
+  CGX_VECTOR_P = 2, /* search direction */
+  CGX_VECTOR_Q = 3, /* A p */
+  CGX_VECTOR_R = 4, /* residual */
+  CGX_VECTOR_Z = 5  /* preconditioned residual */
+} cgx_vector;
+
+/* CG::MatrixFormat (CG.h:38-47). */
+typedef enum cgx_format {
+  CGX_FORMAT_COO = 0,
+  CGX_FORMAT_CRS = 1,
+  CGX_FORMAT_ELL = 2
+} cgx_format;
+
+/* CG::Preconditioner (CG.h:50-55), plus the learned factor G G^T + eps I. */
+typedef enum cgx_preconditioner {
+  CGX_PRECONDITIONER_NONE = 0,
+  CGX_PRECONDITIONER_JACOBI = 1,
+  CGX_PRECONDITIONER_LEARNED = 2
+} cgx_preconditioner;
+
+typedef enum cgx_precision {
+  CGX_PRECISION_FP64 = 0, /* the reference's arithmetic (def.h:6) */
+  CGX_PRECISION_MIXED = 1 /* FP32 inner PCG inside FP64 refinement (CRS) */
+} cgx_precision;
+
+typedef enum cgx_loop {
+  CGX_LOOP_GRAPH = 0,   /* whole solve = one CUDA graph with a while node */
+  CGX_LOOP_CHUNKED = 1, /* graph of a fixed number of iterations, host polls */
+  CGX_LOOP_KERNELS = 2  /* one launch per fused kernel, each timed by events */
+} cgx_loop;
+
+/* Solver settings: the reference's CG_* environment switches
+ * (CG.cpp:35-149) plus this library's own. */
+typedef struct cgx_options {
+  int max_iterations;      /* CG_MAX_ITER, > 0 (CG.h:67, default 1000) */
+  double tolerance;        /* CG_TOLERANCE, > 0 (CG.h:70, default 1e-9) */
+  int preconditioner;      /* cgx_preconditioner (default JACOBI) */
+  int precision;           /* cgx_precision (default FP64) */
+  int loop;                /* cgx_loop (default GRAPH) */
+  double inner_tolerance;  /* MIXED: floor of the inner relative tolerance */
+  int max_outer;           /* MIXED: limit on refinement steps */
+  int compute_true_residual; /* FP64 ||k - A x|| / ||k|| after the solve */
+} cgx_options;
+
+typedef struct cgx_result {
+  int iterations;        /* as printed by CG::printSummary (CG.cpp:424);
+                            MIXED: total inner iterations */
+  double residual;       /* FP64: recurrence residual ||r|| / ||r0||
+                            (CG.cpp:350); MIXED: FP64 true residual */
+  double true_residual;  /* ||k - A x|| / ||k|| in FP64 if requested, else -1 */
+  int converged;         /* residual <= tolerance */
+  int outer_iterations;  /* MIXED: refinement steps; 0 otherwise */
+  double solve_ms;       /* device time of the solve (CUDA events) */
+  /* CGX_LOOP_KERNELS only: device time per fused kernel class (ms) and the
+   * number of launches of each; zero in the other loop modes. */
+  double spmv_ms, update_ms, direction_ms;
+  int spmv_launches, update_launches, direction_launches;
+  int fell_back;         /* learned preconditioner replaced by Jacobi */
+} cgx_result;
+
+/* Library ------------------------------------------------------------------ */
+
+void cgx_version(int *major, int *minor);
+const char *cgx_status_string(cgx_status s);
+/* Message of the last failed call on this thread ("" if none). */
+const char *cgx_last_error(void);
+/* Number of CUDA devices visible (0 on a machine without a GPU). */
+cgx_status cgx_device_count(int *count);
+cgx_status cgx_default_options(cgx_options *opts);
+
+/* Handle: replaces the device bookkeeping of CGCUDABase::Device
+ * (cuda/CGCUDABase.h:17-90) and checkedSetDevice(0) in CGCUDA::init
+ * (cuda/CGCUDA.cu:29-36). `device` is a CUDA ordinal. */
+cgx_status cgx_create(cgx_handle **out, int device);
+cgx_status cgx_destroy(cgx_handle *h);
+/* Uses an existing cudaStream_t (passed as void*) for all work; NULL
+ * restores the handle's own stream. */
+cgx_status cgx_set_stream(cgx_handle *h, void *stream);
+cgx_status cgx_synchronize(cgx_handle *h);
+
+/* Data transfer: CGCUDA::doTransferTo (cuda/CGCUDA.cu:38-75) and
+ * CGCUDABase::allocateAndCopyMatrixDataCRS/ELL (cuda/CGCUDABase.cu:5-37).
+ * Uploading a matrix (re)allocates every device vector for its N; K, X are
+ * zeroed. Arrays are validated (ptr monotone from 0 to nz, indices in
+ * [0, N)); invalid data returns CGX_ERROR_INVALID_ARGUMENT. */
+cgx_status cgx_upload_crs(cgx_handle *h, int N, int nz, const int *ptr,
+                          const int *index, const double *value);
+/* ELL as in MatrixDataELL (Matrix.h:74-87): column-major, element (i, j) at
+ * j*N + i, length[i] entries used per row, maxNz slots per row. */
+cgx_status cgx_upload_ell(cgx_handle *h, int N, int nz, int maxNz,
+                          const int *length, const int *index,
+                          const double *data);
+/* COO as in MatrixCOO (Matrix.h:22-31), entries in file order. */
+cgx_status cgx_upload_coo(cgx_handle *h, int N, int nz, const int *I,
+                          const int *J, const double *V);
+/* Jacobi::C (Preconditioner.h:12-25), N doubles. */
+cgx_status cgx_upload_jacobi(cgx_handle *h, const double *C);
+/* Computes C[i] = 1 / A_ii on the device from the uploaded matrix, with the
+ * semantics of Jacobi::init (Preconditioner.cpp:13-23): the last diagonal
+ * entry of a row in file order wins; a row without one gets C = 0. */
+cgx_status cgx_jacobi_from_matrix(cgx_handle *h);
+cgx_status cgx_set_vector(cgx_handle *h, cgx_vector v, const double *host);
+/* CGCUDA::doTransferFrom (cuda/CGCUDA.cu:77-112) for one vector. */
+cgx_status cgx_get_vector(cgx_handle *h, cgx_vector v, double *host);
+cgx_status cgx_fill_vector(cgx_handle *h, cgx_vector v, double value);
+cgx_status cgx_matrix_info(cgx_handle *h, int *N, int *nz, int *format);
+
+/* Per-kernel interface, one entry per pure virtual of CG (CG.h:224-237),
+ * operating on the device-resident vectors. */
+cgx_status cgx_copy(cgx_handle *h, cgx_vector dst, cgx_vector src); /* cpy */
+cgx_status cgx_matvec(cgx_handle *h, cgx_vector x, cgx_vector y);   /* y = A x */
+cgx_status cgx_axpy(cgx_handle *h, double a, cgx_vector x,
+                    cgx_vector y);                                 /* y += a x */
+cgx_status cgx_xpay(cgx_handle *h, cgx_vector x, double a,
+                    cgx_vector y);                          /* y = x + a y */
+cgx_status cgx_dot(cgx_handle *h, cgx_vector a, cgx_vector b,
+                   double *result);                         /* <a, b> */
+cgx_status cgx_apply_jacobi(cgx_handle *h, cgx_vector x,
+                            cgx_vector y); /* y = C o x */
+
+/* CG::solve (CG.cpp:284-385) as one device-resident solve: r = k - A x,
+ * then PCG until ||r|| / ||r0|| <= tolerance or max_iterations, with every
+ * scalar kept on the device. Starts from the current X (the reference's
+ * resetX sets it to 0, CG.cpp:272-275) and leaves the solution in X. */
+cgx_status cgx_solve(cgx_handle *h, const cgx_options *opts,
+                     cgx_result *result);
+
+/* FP64 ||k - A x|| / ||k|| of the current X. */
+cgx_status cgx_true_residual(cgx_handle *h, double *rel);
+
+/* MatrixMarket I/O (MatrixCOO::MatrixCOO, Matrix.cpp:13-111). Reads a
+ * `matrix coordinate real general|symmetric` file into newly malloc'ed
+ * arrays (free them with cgx_free) with the reference's entry order:
+ * symmetric off-diagonal entries are mirrored into the next slot. The file
+ * is parsed by several host threads. Returns CGX_ERROR_IO with the
+ * reference's message on the conditions where it calls exit(1). */
+cgx_status cgx_mtx_read(const char *path, int *N, int *nz, int **I, int **J,
+                        double **V);
+/* Writes the lower triangle (row >= col) of a CRS matrix as a symmetric
+ * MatrixMarket file with 17 significant digits (round-trips exactly). */
+cgx_status cgx_mtx_write_symmetric_crs(const char *path, int N,
+                                       const int *ptr, const int *index,
+                                       const double *value);
+void cgx_free(void *p);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CGX_H */

@@ -1,0 +1,148 @@
+"""Parity of the fused device solve (cgx_solve) with the oracle's CG::solve.
+
+Bar (from the project's goal): the solution's relative difference to the
+oracle's is <= 1e-8, the iteration count is within 2 %, and the reference's
+CG_CHECK_TOLERANCE check (|x_i - 1| <= 1e-5 for k = A*1) passes.
+"""
+import numpy as np
+import pytest
+
+import cgxx_b200 as cg
+from cgxx_b200 import generators as G
+from conftest import random_crs
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+X_TOL = 1e-8
+
+
+def rel(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+def upload(h, A, fmt):
+    if fmt == "CRS":
+        h.upload_crs(A.ptr, A.index, A.value)
+    elif fmt == "ELL":
+        m, l, i, d = G.to_ell(A)
+        h.upload_ell(A.N, A.nz, m, l, i, d)
+    else:
+        I, J, V = G.symmetric_file_coo(A)
+        h.upload_coo(A.N, I, J, V)
+
+
+def solve_case(h, A, k, fmt="CRS", precond="jacobi", loop=cg.LOOP_GRAPH, max_iter=1000,
+               tol=1e-9):
+    upload(h, A, fmt)
+    Cd = 1.0 / A.diagonal()
+    if precond == "jacobi":
+        h.upload_jacobi(Cd)
+    h.set_vector("K", k)
+    h.fill_vector("X", 0.0)
+    pc = cg.PRECOND_JACOBI if precond == "jacobi" else cg.PRECOND_NONE
+    res = h.solve(max_iterations=max_iter, tolerance=tol, preconditioner=pc, loop=loop)
+    x = h.get_vector("X")
+    xo, ito, reso = O.cg_solve_crs(A.ptr, A.index, A.value, k,
+                                   Cd if precond == "jacobi" else None,
+                                   max_iter=max_iter, tol=tol)
+    return res, x, xo, ito, reso
+
+
+@pytest.mark.parametrize("loop", [cg.LOOP_GRAPH, cg.LOOP_CHUNKED, cg.LOOP_KERNELS])
+@pytest.mark.parametrize("fmt", ["CRS", "ELL", "COO"])
+def test_poisson256_matches_reference(handle, fmt, loop):
+    A = G.poisson2d(256)
+    k = G.rhs_ones(A)
+    res, x, xo, ito, reso = solve_case(handle, A, k, fmt=fmt, loop=loop)
+    assert ito == 482  # the reference's cg_serial on this matrix
+    assert abs(res["iterations"] - ito) <= 0.02 * ito
+    assert res["converged"] == 1
+    assert res["residual"] <= 1e-9
+    assert rel(x, xo) <= X_TOL
+    assert np.sum(np.abs(x - 1.0) > 1e-5) == 0  # CG::check
+
+
+@pytest.mark.parametrize("precond", ["jacobi", "none"])
+@pytest.mark.parametrize("N", [1, 2, 33, 1000, 20000])
+def test_random_spd(handle, N, precond):
+    A = random_crs(N, 0, 40, seed=N, spd=True)
+    b, xs = G.rhs_for(A, seed=N)
+    res, x, xo, ito, reso = solve_case(handle, A, b, precond=precond, max_iter=5000)
+    assert abs(res["iterations"] - ito) <= max(1, 0.02 * ito)
+    assert rel(x, xo) <= X_TOL
+
+
+@pytest.mark.parametrize("stencil", [7, 27])
+def test_diffusion3d(handle, stencil):
+    A = G.diffusion3d(24, stencil=stencil, sigma=1.0, corr_len=4.0, seed=3)
+    b, xs = G.rhs_for(A, seed=4)
+    for fmt in ("CRS", "ELL"):
+        res, x, xo, ito, reso = solve_case(handle, A, b, fmt=fmt, max_iter=3000)
+        assert abs(res["iterations"] - ito) <= max(1, 0.02 * ito)
+        assert rel(x, xo) <= X_TOL
+        assert rel(x, xs) <= 1e-6
+
+
+def test_iteration_limit(handle):
+    A = G.poisson2d(64)
+    k = G.rhs_ones(A)
+    for loop in (cg.LOOP_GRAPH, cg.LOOP_CHUNKED, cg.LOOP_KERNELS):
+        res, x, xo, ito, reso = solve_case(handle, A, k, max_iter=17, loop=loop)
+        assert res["iterations"] == 17 == ito
+        assert res["converged"] == 0
+        assert rel(x, xo) <= 1e-10
+        assert abs(res["residual"] - reso) <= 1e-8 * reso
+
+
+def test_repeat_solve_is_deterministic(handle):
+    A = G.diffusion3d(20, stencil=7, seed=9)
+    b, _ = G.rhs_for(A, seed=1)
+    r1, x1, *_ = solve_case(handle, A, b)
+    handle.fill_vector("X", 0.0)
+    r2 = handle.solve(max_iterations=1000, tolerance=1e-9)
+    x2 = handle.get_vector("X")
+    assert r1["iterations"] == r2["iterations"]
+    assert np.array_equal(x1, x2)
+
+
+def test_mixed_precision_reaches_fp64_tolerance(handle):
+    A = G.diffusion3d(32, stencil=7, sigma=1.0, corr_len=8.0, seed=2)
+    b, xs = G.rhs_for(A, seed=2)
+    handle.upload_crs(A.ptr, A.index, A.value)
+    Cd = 1.0 / A.diagonal()
+    handle.upload_jacobi(Cd)
+    handle.set_vector("K", b)
+    handle.fill_vector("X", 0.0)
+    res = handle.solve(max_iterations=5000, tolerance=1e-9, precision=cg.PRECISION_MIXED)
+    x = handle.get_vector("X")
+    assert res["converged"] == 1
+    assert res["outer_iterations"] >= 2
+    # FP64 true residual computed independently on the CPU.
+    tr = np.linalg.norm(b - A.matvec(x)) / np.linalg.norm(b)
+    assert tr <= 1e-9
+    # Error against a tight FP64 oracle solve.
+    xo, _, _ = O.cg_solve_crs(A.ptr, A.index, A.value, b, Cd, max_iter=20000, tol=1e-13)
+    assert rel(x, xo) <= 1e-6
+    # Oracle of the mixed scheme: same number of refinement steps, inner
+    # iteration total within 5 %.
+    _, it_o, outer_o, tr_o = O.mixed_ir_solve(A.ptr, A.index, A.value, Cd, b)
+    assert res["outer_iterations"] == outer_o
+    assert abs(res["iterations"] - it_o) <= 0.05 * it_o + 2
+
+
+def test_mixed_loops_agree(handle):
+    A = G.diffusion3d(16, stencil=27, seed=5)
+    b, _ = G.rhs_for(A, seed=3)
+    handle.upload_crs(A.ptr, A.index, A.value)
+    handle.upload_jacobi(1.0 / A.diagonal())
+    handle.set_vector("K", b)
+    out = []
+    for loop in (cg.LOOP_GRAPH, cg.LOOP_CHUNKED, cg.LOOP_KERNELS):
+        handle.fill_vector("X", 0.0)
+        r = handle.solve(max_iterations=5000, tolerance=1e-9, precision=cg.PRECISION_MIXED,
+                         loop=loop)
+        out.append((r["iterations"], handle.get_vector("X")))
+        assert r["converged"] == 1
+    assert out[0][0] == out[1][0] == out[2][0]
+    assert np.array_equal(out[0][1], out[1][1]) and np.array_equal(out[0][1], out[2][1])
