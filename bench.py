@@ -1,0 +1,485 @@
+#!/usr/bin/env python3
+"""Benchmark: milliseconds to a 1e-9 relative residual on one B200.
+
+Workload (default): 3-D 7-point variable-coefficient diffusion on a 160^3
+grid (N = 4,096,000, nnz = 28,518,400), face coefficients exp(g) with g a
+seeded Gaussian random field (sigma 1, correlation length 8 cells), FP64
+values in CRS, Jacobi preconditioner, b = A x* with x* ~ U[-1, 1], tolerance
+1e-9. Synthetic and seeded: the reference ships no matrices.
+
+One step = one complete solve from x0 = 0 to the tolerance, inputs resident
+in device memory. The matrix (342 MB) is larger than the 126 MB L2, so no
+flush is needed between steps.
+
+Paths (--path): plain = FP64 Jacobi-PCG (the reference's arithmetic),
+mixed = FP32 inner Jacobi-PCG inside FP64 iterative refinement (stops on the
+FP64 true residual). `value` is the solve time of the path named in
+config.path; the other path's time is reported next to it.
+
+--impl reference runs the reference's own OpenMP CG (oracle/_ref, built from
+the unmodified reference sources) on the box's host cores instead.
+
+Prints one JSON line (rank 0).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = "ms to 1e-9 rel. residual: learned-precond mixed CG vs plain FP64 Jacobi CG"
+CACHE = os.path.join(tempfile.gettempdir(), "cgxx_b200_bench")
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=160, help="grid edge (default 160)")
+    ap.add_argument("--path", choices=["plain", "mixed"], default="plain")
+    ap.add_argument("--max-iter", type=int, default=5000)
+    ap.add_argument("--tol", type=float, default=1e-9)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--loop", choices=["graph", "chunked", "kernels"], default="graph",
+                    help="device loop of the timed solves (profilers need kernels: "
+                         "they cannot see inside a graph with a while node)")
+    ap.add_argument("--quick", action="store_true",
+                    help="timed solves only (for profiler runs): no other path, "
+                         "no per-kernel pass, no e2e, no CPU baseline")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# Distributed plumbing (one process per GPU; replicas, no data exchange)
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(world, v):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(v)], device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------
+# Workload
+
+def workload(n):
+    from cgxx_b200 import generators as G
+    A = G.diffusion3d(n, stencil=7, sigma=1.0, corr_len=8.0, seed=2024)
+    b, xs = G.rhs_for(A, seed=7)
+    return A, b, xs
+
+
+def workload_config(args, A):
+    return {
+        "workload": f"diffusion3d-7pt-{args.n}^3",
+        "N": A.N, "nnz": A.nz, "format": "CRS", "preconditioner": "jacobi",
+        "path": args.path, "field": "exp(GRF sigma=1, corr_len=8 cells), seed 2024",
+        "rhs": "A x*, x* ~ U[-1,1] seed 7", "tolerance": args.tol,
+        "max_iterations": args.max_iter, "l2": "inputs larger than L2 (no flush)",
+        "parallelism": "replicas" if args.gpus > 1 else "single GPU",
+    }
+
+
+# ---------------------------------------------------------------------------
+# Clocks during the timed region
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            with open(self.path) as f:
+                for line in f:
+                    parts = [p.strip() for p in line.split(",")]
+                    if len(parts) >= 9:
+                        rows.append(parts)
+        except Exception:
+            pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for nm, v in zip(names, r[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# Reference CPU implementation (oracle/_ref, built from the reference sources)
+
+def mtx_cache_path(A, n):
+    os.makedirs(CACHE, exist_ok=True)
+    path = os.path.join(CACHE, f"diffusion7_{n}.mtx")
+    if not os.path.exists(path):
+        tmp = path + f".tmp{os.getpid()}"
+        from cgxx_b200 import generators as G
+        G.write_mtx_symmetric(tmp, A)
+        os.replace(tmp, path)
+    return path
+
+
+def run_reference(A, b, n, reps, max_iter, tol, threads):
+    """Runs the reference's OpenMP CG in-process harness on the workload with
+    right-hand side b. Returns the list of per-repetition solve times (s) and
+    the iteration counts."""
+    from oracle import oracle as O
+    path = mtx_cache_path(A, n)
+    env = {"CG_MAX_ITER": str(max_iter), "CG_TOLERANCE": repr(tol),
+           "CG_MATRIX_FORMAT": "CRS", "CG_PRECONDITIONER": "jacobi",
+           "OMP_NUM_THREADS": str(threads), "OMP_PROC_BIND": "spread"}
+    summ, x = O.run_ref_harness(path, rhs=b, backend="omp", reps=reps, env=env)
+    return summ["solve_time"], summ["iterations"], x
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def reference_arm(args, world, rank):
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    if O.ref_binary("ref_harness_omp") is None:
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "oracle/_ref/ref_harness_omp was not built (reference sources absent)"}))
+        return
+    A, b, _ = workload(args.n)
+    threads = host_threads()
+    # Warm-up repetitions are full solves; they also give the iteration count
+    # and the time of one full solve.
+    wt, witers, _ = run_reference(A, b, args.n, max(1, args.warmup), args.max_iter,
+                                  args.tol, threads)
+    full_iters, full_s = witers[-1], min(wt)
+    if full_s * args.steps <= 240.0:
+        times, iters, _ = run_reference(A, b, args.n, args.steps, args.max_iter, args.tol,
+                                        threads)
+        ms = 1e3 * sum(times) / len(times)
+        sample = (f"{args.steps} full solves ({iters[-1]} iterations) by the reference's "
+                  f"CGOpenMP, OMP_NUM_THREADS={threads}")
+    else:
+        # Bounded sample: each step runs `cap` iterations; the time is scaled
+        # to the full iteration count.
+        cap = max(10, int(full_iters * 240.0 / (full_s * args.steps)))
+        times, iters, _ = run_reference(A, b, args.n, args.steps, cap, args.tol, threads)
+        ms = 1e3 * (sum(times) / len(times)) * full_iters / iters[-1]
+        sample = (f"{args.steps} solves capped at {iters[-1]} iterations (CG_MAX_ITER), "
+                  f"scaled to the full {full_iters}; CGOpenMP, OMP_NUM_THREADS={threads}")
+    iters = [full_iters]
+    line = {
+        "metric": METRIC, "value": ms, "unit": "ms", "impl": "reference",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": dict(workload_config(args, A), path="reference OpenMP Jacobi-CG (CRS)"),
+        "iterations": iters[-1],
+        "cpu_baseline": {"value": ms, "unit": "ms", "cores": threads, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+# ---------------------------------------------------------------------------
+# Our arm
+
+def read_traffic_profile(name):
+    p = os.path.join(REPO, "profiles", name)
+    try:
+        with open(p) as f:
+            return json.load(f)
+    except Exception:
+        return None
+
+
+def peaks():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+LOOPS = {"graph": 0, "chunked": 1, "kernels": 2}
+
+
+def solve_opts(cg, args, path, loop=None):
+    return cg.default_options(
+        max_iterations=args.max_iter, tolerance=args.tol,
+        preconditioner=cg.PRECOND_JACOBI,
+        precision=cg.PRECISION_MIXED if path == "mixed" else cg.PRECISION_FP64,
+        loop=LOOPS[args.loop] if loop is None else loop, inner_tolerance=1e-5, max_outer=30)
+
+
+def our_arm(args, world, rank, local):
+    import torch
+
+    import cgxx_b200 as cg
+
+    A, b, xs = workload(args.n)
+    Cd = 1.0 / A.diagonal()
+    dev = local if world > 1 else 0
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream()
+    h = cg.Handle(dev)
+    h.set_stream(stream.cuda_stream)
+    h.upload_crs(A.ptr, A.index, A.value)
+    h.upload_jacobi(Cd)
+    h.set_vector("K", b)
+
+    def one_solve(path):
+        h.fill_vector("X", 0.0)
+        return h.solve(solve_opts(cg, args, path))
+
+    # Warm-up (also builds the CUDA graphs of both paths).
+    for _ in range(args.warmup):
+        one_solve(args.path)
+    other = "mixed" if args.path == "plain" else "plain"
+    if not args.quick:
+        one_solve(other)
+
+    # Timed region: K complete solves, device-timed with CUDA events on the
+    # stream the library launches on, bracketed by barrier + synchronize.
+    results = []
+    with ClockSampler(dev) as clk:
+        barrier(world)
+        torch.cuda.synchronize()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(args.steps):
+            results.append(one_solve(args.path))
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        barrier(world)
+    ms = ev0.elapsed_time(ev1) / args.steps
+    ms = max_over_ranks(world, ms)
+    clocks = clk.summary()
+    res = results[-1]
+    x = h.get_vector("X")
+    true_rel = float(np.linalg.norm(b - A.matvec(x)) / np.linalg.norm(b))
+    err_vs_exact = float(np.linalg.norm(x - xs) / np.linalg.norm(xs))
+    if args.quick:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": ms, "unit": "ms", "quick": True,
+                              "iterations": res["iterations"], "true_residual": true_rel,
+                              "config": workload_config(args, A), "clocks": clocks}))
+        h.close()
+        return
+
+    # The other path, for the side-by-side number.
+    oth = []
+    for _ in range(2):
+        oth.append(one_solve(other))
+    other_ms = statistics.median(r["solve_ms"] for r in oth)
+
+    # Per-launch kernel times (roofline): one solve of the plain path with
+    # every fused kernel bracketed by CUDA events.
+    h.fill_vector("X", 0.0)
+    kr = h.solve(solve_opts(cg, args, "plain", loop=cg.LOOP_KERNELS))
+    spmv_us = 1e3 * kr["spmv_ms"] / max(1, kr["spmv_launches"])
+    upd_us = 1e3 * kr["update_ms"] / max(1, kr["update_launches"])
+    dir_us = 1e3 * kr["direction_ms"] / max(1, kr["direction_launches"])
+    N, nnz = A.N, A.nz
+    spmv_bytes = 12 * nnz + 4 * (N + 1) + 16 * N   # values+cols, ptr, p once, q
+    upd_bytes = 32 * N                              # r, q, C read; r written
+    dir_bytes = 48 * N                              # x, p, r, C read; x, p written
+    iter_bytes = spmv_bytes + upd_bytes + dir_bytes
+    peak, peak_kind = peaks()
+    achieved = spmv_bytes / (spmv_us * 1e-6) / 1e9
+    iter_us = spmv_us + upd_us + dir_us
+    prof = read_traffic_profile("spmv_crs_fp64_diffusion7_160.json")
+    traffic = prof.get("dram_bytes_per_launch") if prof else None
+
+    # End to end through the public C ABI: pinned host inputs uploaded every
+    # step (matrix, Jacobi C, right-hand side), solve, read back x.
+    ptr_h = cg.pinned_empty(N + 1, np.int32)
+    idx_h = cg.pinned_empty(nnz, np.int32)
+    val_h = cg.pinned_empty(nnz, np.float64)
+    b_h = cg.pinned_empty(N, np.float64)
+    c_h = cg.pinned_empty(N, np.float64)
+    x_h = cg.pinned_empty(N, np.float64)
+    ptr_h[:] = A.ptr
+    idx_h[:] = A.index
+    val_h[:] = A.value
+    b_h[:] = b
+    c_h[:] = Cd
+    e2e_steps = max(2, min(args.steps, 5))
+
+    def e2e_step():
+        h.upload_crs(ptr_h, idx_h, val_h)
+        h.upload_jacobi(c_h)
+        h.set_vector("K", b_h)
+        r = h.solve(solve_opts(cg, args, args.path))
+        out = h.get_vector("X")
+        x_h[:] = out
+        return r
+
+    e2e_step()  # warm-up (graph build after re-upload)
+    barrier(world)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    wall_ms = (time.perf_counter() - t0) * 1e3 / e2e_steps
+    barrier(world)
+    e2e_ms = max_over_ranks(world, wall_ms)
+    h2d = 4 * (N + 1) + 12 * nnz + 16 * N
+    d2h = 8 * N
+
+    iters = res["iterations"]
+    if args.path == "plain":
+        launches = args.steps * (1 + 1 + 4 * iters)  # fill, setup, 3 fused + guard
+    else:
+        outer = res["outer_iterations"]
+        launches = args.steps * (1 + 1 + (outer + 1) + outer * 2 + 4 * iters)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(A, b, args, iters if args.path == "plain" else None)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": ms, "unit": "ms", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.path == "plain" else "f32+f64",
+            "data": "synthetic (seeded generator; no dataset)",
+            "config": workload_config(args, A),
+            "iterations": iters, "outer_iterations": res["outer_iterations"],
+            "residual": res["residual"], "true_residual": true_rel,
+            "rel_error_vs_exact": err_vs_exact, "converged": bool(res["converged"]),
+            "other_path": {"path": other, "ms": other_ms,
+                           "iterations": oth[-1]["iterations"]},
+            "kernel_us": {"spmv_fused_dot": spmv_us, "update": upd_us,
+                          "direction": dir_us, "iteration": iter_us},
+            "iteration_gbs": iter_bytes / (iter_us * 1e-6) / 1e9,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                         "kernel": "k_crs<double, OpPcgQ> (q = A p fused with <p,q>)",
+                         "algorithmic_bytes": spmv_bytes, "peak_kind": peak_kind},
+            "clocks": clocks,
+            "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "steps": e2e_steps},
+            "gpu_launches": launches,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+    h.close()
+
+
+def cpu_baseline(A, b, args, full_iters):
+    """The reference's OpenMP CG on a bounded sample: `sample` iterations of
+    the same solve (CG_MAX_ITER), scaled to the full iteration count."""
+    from oracle import oracle as O
+    if O.ref_binary("ref_harness_omp") is None:
+        return None
+    threads = host_threads()
+    sample = 100
+    try:
+        times, iters, _ = run_reference(A, b, args.n, 2, sample, args.tol, threads)
+    except Exception as e:  # pragma: no cover - reported, not fatal
+        return {"value": None, "error": str(e)[:200]}
+    t = min(times)
+    per_iter_ms = 1e3 * t / iters[-1]
+    full = full_iters or iters[-1]
+    return {"value": per_iter_ms * full, "unit": "ms", "cores": threads, "kind": "reference",
+            "sample": f"{iters[-1]} iterations (CG_MAX_ITER={sample}) of the same solve by the "
+                      f"reference's CGOpenMP, best of 2, scaled to {full} iterations",
+            "ms_per_iteration": per_iter_ms}
+
+
+def main():
+    args = parse_args()
+    world, rank, local = dist_setup(args)
+    args.gpus = world if world > 1 else args.gpus
+    try:
+        if args.impl == "reference":
+            reference_arm(args, world, rank)
+        else:
+            our_arm(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -10,7 +10,7 @@ missing.
 """
 from ._lib import (  # noqa: F401
     CgxError, Handle, default_options, device_count, load, mtx_read,
-    mtx_write_symmetric_crs,
+    mtx_write_symmetric_crs, pinned_empty,
     FORMAT_COO, FORMAT_CRS, FORMAT_ELL,
     PRECOND_NONE, PRECOND_JACOBI, PRECOND_LEARNED,
     PRECISION_FP64, PRECISION_MIXED,

@@ -106,6 +106,8 @@ PROTOTYPES = {
                      C.POINTER(_PD)],
     "cgx_mtx_write_symmetric_crs": [C.c_char_p, _I, _P, _P, _P],
     "cgx_free": [_P],
+    "cgx_host_alloc": [C.POINTER(_P), C.c_size_t],
+    "cgx_host_free": [_P],
 }
 _RESTYPE = {"cgx_version": None, "cgx_status_string": C.c_char_p,
             "cgx_last_error": C.c_char_p, "cgx_free": None}
@@ -251,6 +253,11 @@ class Handle:
     def synchronize(self):
         check(self._lib.cgx_synchronize(self._h))
 
+    def set_stream(self, stream_ptr):
+        """Run all work on an existing cudaStream_t (an int handle, e.g.
+        torch.cuda.Stream().cuda_stream); 0/None restores the own stream."""
+        check(self._lib.cgx_set_stream(self._h, C.c_void_p(stream_ptr or None)))
+
     # --- solve (CG::solve) ---
     def solve(self, options=None, **kw):
         o = options if options is not None else default_options(**kw)
@@ -262,6 +269,36 @@ class Handle:
         r = C.c_double()
         check(self._lib.cgx_true_residual(self._h, C.byref(r)))
         return r.value
+
+
+def pinned_empty(n, dtype):
+    """numpy array of n elements in page-locked host memory (cgx_host_alloc);
+    the memory is released when the array is garbage collected."""
+    dt = np.dtype(dtype)
+    lib = load()
+    p = C.c_void_p()
+    check(lib.cgx_host_alloc(C.byref(p), max(1, n * dt.itemsize)))
+    buf = (C.c_byte * max(1, n * dt.itemsize)).from_address(p.value)
+    arr = np.frombuffer(buf, dtype=dt, count=n)
+
+    class _Owner:
+        def __init__(self, ptr):
+            self.ptr = ptr
+
+        def __del__(self):
+            try:
+                lib.cgx_host_free(self.ptr)
+            except Exception:
+                pass
+
+    # keep the owner alive as long as the array
+    arr = arr.view(type=_PinnedArray)
+    arr._owner = _Owner(p)
+    return arr
+
+
+class _PinnedArray(np.ndarray):
+    _owner = None
 
 
 def mtx_read(path):

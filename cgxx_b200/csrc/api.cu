@@ -631,6 +631,18 @@ cgx_status cgx_synchronize(cgx_handle *h) {
   return CGX_SUCCESS;
 }
 
+cgx_status cgx_host_alloc(void **p, size_t bytes) {
+  if (!p) return fail(CGX_ERROR_INVALID_ARGUMENT, "p is NULL");
+  *p = nullptr;
+  CUDA_TRY(cudaMallocHost(p, bytes > 0 ? bytes : 1));
+  return CGX_SUCCESS;
+}
+
+cgx_status cgx_host_free(void *p) {
+  if (p) CUDA_TRY(cudaFreeHost(p));
+  return CGX_SUCCESS;
+}
+
 cgx_status cgx_matrix_info(cgx_handle *h, int *N, int *nz, int *format) {
   if (!h) return fail(CGX_ERROR_INVALID_ARGUMENT, "handle is NULL");
   if (N) *N = h->N;

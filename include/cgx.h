@@ -196,6 +196,12 @@ cgx_status cgx_mtx_write_symmetric_crs(const char *path, int N,
                                        const double *value);
 void cgx_free(void *p);
 
+/* Page-locked host memory for vectors that cross the boundary every solve
+ * (the reference pins x: CGCUDABase::allocateX, cuda/CGCUDABase.h:101-104).
+ * Free with cgx_host_free. */
+cgx_status cgx_host_alloc(void **p, size_t bytes);
+cgx_status cgx_host_free(void *p);
+
 #ifdef __cplusplus
 }
 #endif

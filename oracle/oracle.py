@@ -64,6 +64,10 @@ def load():
         lib.orc_coo_free.argtypes = [C.POINTER(_Coo)]
         lib.orc_check_ones.argtypes = [C.c_int, P, C.c_double]
         lib.orc_check_ones.restype = C.c_int
+        lib.orc_coo_to_crs.argtypes = [C.POINTER(_Coo), P, P, P]
+        lib.orc_coo_to_ell.argtypes = [C.POINTER(_Coo), C.c_int, P, P, P]
+        lib.orc_jacobi_init.argtypes = [C.POINTER(_Coo), P]
+        lib.orc_rhs_ones.argtypes = [C.POINTER(_Coo), P]
         _lib = lib
     return _lib
 
@@ -240,3 +244,56 @@ def run_ref_harness(mtx, rhs=None, backend="serial", reps=1, env=None, x_out=Non
             raise RuntimeError(f"{cmd} failed: {p.stderr}")
         x = np.fromfile(xp, dtype=np.float64)
         return parse_summary(p.stdout), x
+
+
+def coo_to_crs(N, I, J, V):
+    """DataMatrix<CRS>::convert restated (Matrix.cpp:203-228)."""
+    lib = load()
+    c = _coo_struct(N, I, J, V)
+    ptr = np.empty(N + 1, np.int32)
+    index = np.empty(max(1, len(I)), np.int32)
+    value = np.empty(max(1, len(I)), np.float64)
+    lib.orc_coo_to_crs(C.byref(c[0]), _p(ptr), _p(index), _p(value))
+    return ptr, index[:len(I)], value[:len(I)]
+
+
+def coo_to_ell(N, I, J, V):
+    """DataMatrix<ELL>::convert restated (Matrix.cpp:339-361); padding 0."""
+    lib = load()
+    c = _coo_struct(N, I, J, V)
+    max_nz = int(np.bincount(I, minlength=N).max()) if len(I) else 0
+    length = np.empty(N, np.int32)
+    index = np.zeros(max(1, max_nz * N), np.int32)
+    data = np.zeros(max(1, max_nz * N), np.float64)
+    lib.orc_coo_to_ell(C.byref(c[0]), max_nz, _p(length), _p(index), _p(data))
+    return max_nz, length, index[:max_nz * N], data[:max_nz * N]
+
+
+def jacobi_init(N, I, J, V):
+    """Jacobi::init restated (Preconditioner.cpp:13-23), C zero-initialised."""
+    lib = load()
+    c = _coo_struct(N, I, J, V)
+    Cd = np.zeros(N)
+    lib.orc_jacobi_init(C.byref(c[0]), _p(Cd))
+    return Cd
+
+
+def rhs_ones(N, I, J, V):
+    """k = A * 1 in COO order (CG.cpp:256-261)."""
+    lib = load()
+    c = _coo_struct(N, I, J, V)
+    k = np.empty(N)
+    lib.orc_rhs_ones(C.byref(c[0]), _p(k))
+    return k
+
+
+def _coo_struct(N, I, J, V):
+    I = np.ascontiguousarray(I, np.int32)
+    J = np.ascontiguousarray(J, np.int32)
+    V = np.ascontiguousarray(V, np.float64)
+    nzr = np.bincount(I, minlength=N).astype(np.int32)
+    s = _Coo(N=N, nz=len(I), I=I.ctypes.data_as(C.POINTER(C.c_int)),
+             J=J.ctypes.data_as(C.POINTER(C.c_int)),
+             V=V.ctypes.data_as(C.POINTER(C.c_double)),
+             nzPerRow=nzr.ctypes.data_as(C.POINTER(C.c_int)))
+    return s, (I, J, V, nzr)  # keep the arrays alive with the struct
