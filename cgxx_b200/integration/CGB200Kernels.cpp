@@ -55,8 +55,11 @@ class CGB200Kernels : public CG {
                         matrixCRS->value));
       break;
     case MatrixFormatELL:
-      ok(cgx_upload_ell(h, N, nz, matrixELL->maxNz, matrixELL->length,
-                        matrixELL->index, matrixELL->data));
+      // The reference's conversion sets `elements` (= N * max row length)
+      // but never `maxNz` (Matrix.cpp:339-361), so the width comes from it.
+      ok(cgx_upload_ell(h, N, nz, N > 0 ? matrixELL->elements / N : 0,
+                        matrixELL->length, matrixELL->index,
+                        matrixELL->data));
       break;
     case MatrixFormatCOO:
       ok(cgx_upload_coo(h, N, nz, matrixCOO->I.get(), matrixCOO->J.get(),
