@@ -108,6 +108,7 @@ PROTOTYPES = {
     "cgx_free": [_P],
     "cgx_host_alloc": [C.POINTER(_P), C.c_size_t],
     "cgx_host_free": [_P],
+    "cgx_dot_noalloc": [_P, _P, _I, _P, _P],
 }
 _RESTYPE = {"cgx_version": None, "cgx_status_string": C.c_char_p,
             "cgx_last_error": C.c_char_p, "cgx_free": None}

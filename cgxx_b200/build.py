@@ -21,7 +21,7 @@ EXE = os.path.join(HERE, "cg_b200")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3",
               "--expt-relaxed-constexpr"]
-CU_SOURCES = ["csrc/api.cu"]
+CU_SOURCES = ["csrc/api.cu", "csrc/noalloc.cu"]
 CPP_SOURCES = ["csrc/mtx_io.cpp"]
 HOST_SOURCES = ["host/CG.cpp", "host/Matrix.cpp", "host/CGB200.cpp"]
 

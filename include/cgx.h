@@ -196,6 +196,26 @@ cgx_status cgx_mtx_write_symmetric_crs(const char *path, int N,
                                        const double *value);
 void cgx_free(void *p);
 
+/* Dot product <a, b> of two device vectors of n doubles, written to *result
+ * (device memory), for callers that cannot allocate device memory: code
+ * running under a framework that owns all device memory, or a loop whose
+ * rules forbid allocation after start-up. It needs no handle and calls no
+ * allocating routine; its scratch (one partial sum per 4096-element chunk)
+ * lives in a fixed 512 KiB array in the library image, held by every GPU that
+ * loads the library until exit. Hence n <= 268,435,456; larger n returns
+ * CGX_ERROR_INVALID_ARGUMENT.
+ *   - Works on the calling thread's current device, on `stream` (a
+ *     cudaStream_t; NULL = the legacy default stream); asynchronous.
+ *   - The first call on each device looks up the array's device address
+ *     (cudaGetSymbolAddress); make that first call before any stream capture.
+ *   - All calls share the one array: calls that overlap on the GPU (different
+ *     streams, or several host threads) race and give wrong results.
+ * Deterministic: the result depends only on a, b and n.
+ * Has no counterpart in the reference (its vectorDotKernel reduces into a
+ * cudaMalloc'ed buffer, cuda/CGCUDA.cu:73). */
+cgx_status cgx_dot_noalloc(const double *a, const double *b, int n,
+                           double *result, void *stream);
+
 /* Page-locked host memory for vectors that cross the boundary every solve
  * (the reference pins x: CGCUDABase::allocateX, cuda/CGCUDABase.h:101-104).
  * Free with cgx_host_free. */
