@@ -9,7 +9,7 @@ preconditioner; it loads the in-tree library and fails loudly if it is
 missing.
 """
 from ._lib import (  # noqa: F401
-    CgxError, Handle, default_options, device_count, load, mtx_read,
+    CgxError, Gnn, Handle, default_options, device_count, load, mtx_read,
     mtx_write_symmetric_crs, pinned_empty,
     FORMAT_COO, FORMAT_CRS, FORMAT_ELL,
     PRECOND_NONE, PRECOND_JACOBI, PRECOND_LEARNED,

@@ -109,9 +109,21 @@ PROTOTYPES = {
     "cgx_host_alloc": [C.POINTER(_P), C.c_size_t],
     "cgx_host_free": [_P],
     "cgx_dot_noalloc": [_P, _P, _I, _P, _P],
+    "cgx_gnn_param_count": [],
+    "cgx_gnn_create": [C.POINTER(_P), _I, _P],
+    "cgx_gnn_destroy": [_P],
+    "cgx_gnn_set_params": [_P, _P],
+    "cgx_gnn_get_params": [_P, _P],
+    "cgx_update_crs_values": [_P, _P],
+    "cgx_learned_setup": [_P],
+    "cgx_learned_factor": [_P, _P, _D],
+    "cgx_learned_get_factor": [_P, _PI, _P, _P, _P],
+    "cgx_gnn_loss_grad": [_P, _P, _P, C.c_ulonglong, C.POINTER(C.c_float), _P],
+    "cgx_gnn_train_step": [_P, _P, C.c_ulonglong, C.c_float, C.POINTER(C.c_float)],
 }
 _RESTYPE = {"cgx_version": None, "cgx_status_string": C.c_char_p,
-            "cgx_last_error": C.c_char_p, "cgx_free": None}
+            "cgx_last_error": C.c_char_p, "cgx_free": None,
+            "cgx_gnn_param_count": C.c_int}
 
 _lib = None
 
@@ -270,6 +282,87 @@ class Handle:
         r = C.c_double()
         check(self._lib.cgx_true_residual(self._h, C.byref(r)))
         return r.value
+
+    # --- learned preconditioner ---
+    def update_crs_values(self, value):
+        value, pv = _arr(value, np.float64)
+        check(self._lib.cgx_update_crs_values(self._h, pv))
+
+    def update_crs_values_ptr(self, device_ptr):
+        """Same as update_crs_values with the values in device memory."""
+        check(self._lib.cgx_update_crs_values(self._h, C.c_void_p(device_ptr)))
+
+    def learned_setup(self):
+        check(self._lib.cgx_learned_setup(self._h))
+
+    def learned_factor(self, gnn, eps=0.0):
+        check(self._lib.cgx_learned_factor(self._h, gnn._g, float(eps)))
+
+    def learned_get_factor(self):
+        """(ghat, rows, cols) of the unscaled factor on its pattern."""
+        n = C.c_int()
+        check(self._lib.cgx_learned_get_factor(self._h, C.byref(n), None, None, None))
+        g = np.empty(n.value, np.float32)
+        r = np.empty(n.value, np.int32)
+        c = np.empty(n.value, np.int32)
+        check(self._lib.cgx_learned_get_factor(
+            self._h, C.byref(n), g.ctypes.data_as(C.c_void_p),
+            r.ctypes.data_as(C.c_void_p), c.ctypes.data_as(C.c_void_p)))
+        return g, r, c
+
+
+class Gnn:
+    """Parameters (and Adam state) of the learned preconditioner's network on
+    one device."""
+
+    def __init__(self, device=0, params=None):
+        self._lib = load()
+        self._g = C.c_void_p()
+        self.nparams = self._lib.cgx_gnn_param_count()
+        p = None
+        if params is not None:
+            params = np.ascontiguousarray(params, np.float32)
+            assert params.size == self.nparams
+            p = params.ctypes.data_as(C.c_void_p)
+        check(self._lib.cgx_gnn_create(C.byref(self._g), device, p))
+
+    def close(self):
+        if self._g:
+            check(self._lib.cgx_gnn_destroy(self._g))
+            self._g = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_params(self, params):
+        params = np.ascontiguousarray(params, np.float32)
+        assert params.size == self.nparams
+        check(self._lib.cgx_gnn_set_params(self._g, params.ctypes.data_as(C.c_void_p)))
+
+    def get_params(self):
+        out = np.empty(self.nparams, np.float32)
+        check(self._lib.cgx_gnn_get_params(self._g, out.ctypes.data_as(C.c_void_p)))
+        return out
+
+    def loss_grad(self, handle, probes=None, seed=0):
+        loss = C.c_float()
+        grad = np.empty(self.nparams, np.float32)
+        pp = None
+        if probes is not None:
+            probes = np.ascontiguousarray(probes, np.float32)
+            pp = probes.ctypes.data_as(C.c_void_p)
+        check(self._lib.cgx_gnn_loss_grad(self._g, handle._h, pp, seed, C.byref(loss),
+                                          grad.ctypes.data_as(C.c_void_p)))
+        return loss.value, grad
+
+    def train_step(self, handle, seed, lr):
+        loss = C.c_float()
+        check(self._lib.cgx_gnn_train_step(self._g, handle._h, seed, float(lr),
+                                           C.byref(loss)))
+        return loss.value
 
 
 def pinned_empty(n, dtype):

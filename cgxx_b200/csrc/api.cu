@@ -15,12 +15,14 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
 
 #include "cgx.h"
 #include "kernels.cuh"
+#include "learned.cuh"
 
 using namespace cgx;
 
@@ -153,6 +155,43 @@ struct cgx_handle {
 
   std::vector<GraphEntry> graphs;
   cudaEvent_t ev[8] = {};
+
+  // Learned preconditioner (cgx_learned_setup / cgx_learned_factor).
+  struct Learned *L = nullptr;
+};
+
+// Device buffers of the learned preconditioner for one matrix.
+struct Learned {
+  int N = 0, nnz = 0, nnzL = 0, nblocks = 0;
+  void *mem = nullptr;    // graph, factor, activations, inner vectors
+  void *train = nullptr;  // training buffers (allocated on first use)
+  double *dis = nullptr;
+  float *ahat = nullptr, *feat = nullptr;
+  int *nlow = nullptr, *nup = nullptr, *sums = nullptr, *flag = nullptr;
+  int *gptr = nullptr, *gcol = nullptr, *grow = nullptr, *g2a = nullptr;
+  int *tptr = nullptr, *tcol = nullptr, *t2g = nullptr, *g2t = nullptr;
+  float *ghat = nullptr, *gs = nullptr, *gts = nullptr;
+  __nv_bfloat16 *h[4] = {};
+  __nv_bfloat16 *agg[3] = {};
+  float *pre[4] = {};
+  float *o = nullptr;
+  float *y32 = nullptr, *z32 = nullptr;
+  double *xbak = nullptr;
+  // training
+  float *V = nullptr, *T1 = nullptr, *T2 = nullptr, *rho = nullptr;
+  float *dT2 = nullptr, *dT1 = nullptr, *dg = nullptr, *dO = nullptr;
+  float *dh = nullptr, *dh2 = nullptr, *dself = nullptr, *dagg = nullptr,
+        *dpre = nullptr;
+  float *partial = nullptr, *grad = nullptr, *loss = nullptr;
+  float *gtmp = nullptr;  // two reduced [W*W | W] blocks of a layer gradient
+  bool has_factor = false;
+  float eps = 0.f;
+};
+
+struct cgx_gnn {
+  int device = 0;
+  float *params = nullptr, *m = nullptr, *v = nullptr;
+  int step = 0;
 };
 
 static void drop_graphs(cgx_handle *h) {
@@ -163,8 +202,17 @@ static void drop_graphs(cgx_handle *h) {
   h->graphs.clear();
 }
 
+static void free_learned(cgx_handle *h) {
+  if (!h->L) return;
+  if (h->L->mem) cudaFree(h->L->mem);
+  if (h->L->train) cudaFree(h->L->train);
+  delete h->L;
+  h->L = nullptr;
+}
+
 static void free_matrix(cgx_handle *h) {
   drop_graphs(h);
+  free_learned(h);
   if (h->mat_mem) cudaFree(h->mat_mem);
   if (h->vec_mem) cudaFree(h->vec_mem);
   if (h->f32_mem) cudaFree(h->f32_mem);
@@ -190,7 +238,7 @@ static void free_matrix(cgx_handle *h) {
 // flight to saturate HBM, never more CTAs than there is work.
 static int grid_stream(const cgx_handle *h, size_t work_items) {
   size_t need = (work_items + kThreads - 1) / kThreads;
-  size_t g = std::min<size_t>((size_t)h->num_sms * 4, need);
+  size_t g = std::min<size_t>((size_t)h->num_sms * 8, need);
   g = std::min<size_t>(g, kMaxGrid);
   return (int)std::max<size_t>(g, 1);
 }
@@ -250,10 +298,12 @@ __global__ void k_loop_guard(CgState *st) {
 // ---------------------------------------------------------------------------
 // Launch helpers
 
+// Staged CRS SpMV over any CRS view (A itself, or the learned factor's G and
+// G^T, whose rows are subsets of A's rows so A's tile capacity bounds them).
 template <typename VT, typename Op>
-static cudaError_t launch_crs(cgx_handle *h, const VT *value, int cap,
-                              const VT *x, Op op) {
-  CrsView<VT> A{h->ptr, h->index, value, h->N, cap};
+static cudaError_t launch_crs_view(cgx_handle *h, CrsView<VT> A, const VT *x,
+                                   Op op) {
+  const int cap = A.tile_cap;
   const size_t smem = crs_smem_bytes<VT>(cap);
   auto kern = k_crs<VT, Op>;
   if (smem > 48 * 1024) {
@@ -271,6 +321,13 @@ static cudaError_t launch_crs(cgx_handle *h, const VT *value, int cap,
   grid = std::max(grid, 1);
   kern<<<grid, kThreads, smem, h->stream>>>(A, x, op, h->st, h->partials);
   return cudaGetLastError();
+}
+
+template <typename VT, typename Op>
+static cudaError_t launch_crs(cgx_handle *h, const VT *value, int cap,
+                              const VT *x, Op op) {
+  return launch_crs_view<VT, Op>(h, CrsView<VT>{h->ptr, h->index, value, h->N, cap},
+                                 x, op);
 }
 
 template <typename Op>
@@ -705,6 +762,7 @@ cgx_status cgx_upload_crs(cgx_handle *h, int N, int nz, const int *ptr,
     maxTile = std::max(maxTile, ptr[r1] - ptr[r0]);
   }
   h->tile_cap = std::min(maxTile, 4096);
+
   Carver c;
   size_t o_ptr = c.take<int>((size_t)N + 1 + kPad);
   size_t o_idx = c.take<int>((size_t)nz + kPad);
@@ -1138,20 +1196,81 @@ static cgx_status true_residual_r2(cgx_handle *h, double *r2) {
   return CGX_SUCCESS;
 }
 
+// z = G (G^T r) + eps C r with <r,z> (start: also p = z and rho).
+static cudaError_t launch_learned_apply(cgx_handle *h, bool start) {
+  Learned *L = h->L;
+  CrsView<float> GT{L->tptr, L->tcol, L->gts, h->N, h->tile_cap};
+  CrsView<float> Gv{L->gptr, L->gcol, L->gs, h->N, h->tile_cap};
+  cudaError_t e = launch_crs_view<float>(h, GT, h->r32, OpInnerStore{L->y32});
+  if (e != cudaSuccess) return e;
+  return launch_crs_view<float>(
+      h, Gv, L->y32,
+      OpLearnedZ{h->r32, h->C32, L->z32, h->p32, L->eps, start ? 1 : 0,
+                 ticket(h, kTicketInnerStart)});
+}
+
+static cudaError_t launch_learned_start(cgx_handle *h) {
+  k_inner_start_z<<<grid_stream(h, h->N), kThreads, 0, h->stream>>>(
+      h->N, h->r64, h->r32, h->d32, h->st, h->partials,
+      ticket(h, kTicketInnerStart));
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  return launch_learned_apply(h, true);
+}
+
+static cudaError_t launch_learned_iteration(cgx_handle *h,
+                                            cudaEvent_t *evs = nullptr) {
+  cudaError_t e;
+  if (evs) cudaEventRecord(evs[0], h->stream);
+  e = launch_crs<float, OpInnerQ>(
+      h, h->value32, h->tile_cap, h->p32,
+      OpInnerQ{h->p32, h->q32, ticket(h, kTicketInnerQ)});
+  if (e != cudaSuccess) return e;
+  if (evs) cudaEventRecord(evs[1], h->stream);
+  const int g = grid_stream(h, h->N);
+  k_inner_update_z<<<g, kThreads, 0, h->stream>>>(
+      h->N, h->r32, h->q32, h->st, h->partials, ticket(h, kTicketInnerUpdate));
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if ((e = launch_learned_apply(h, false)) != cudaSuccess) return e;
+  if (evs) cudaEventRecord(evs[2], h->stream);
+  k_inner_direction_z<<<g, kThreads, 0, h->stream>>>(h->N, h->d32, h->p32,
+                                                     h->L->z32, h->st);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if (evs) cudaEventRecord(evs[3], h->stream);
+  return cudaSuccess;
+}
+
+// FP32-inner / FP64-refinement solve. The inner preconditioner is Jacobi or
+// the learned factor; with the learned one, an outer step whose FP64 true
+// residual is NaN/Inf or shrinks by less than half is undone (x restored) and
+// the remaining steps use Jacobi (result.fell_back = 1).
 static cgx_status solve_mixed(cgx_handle *h, const cgx_options &o,
                               cgx_result &res) {
   if (h->format != CGX_FORMAT_CRS)
     return fail(CGX_ERROR_UNSUPPORTED, "mixed precision needs CRS");
-  if (o.preconditioner != CGX_PRECONDITIONER_JACOBI)
+  const bool want_learned = o.preconditioner == CGX_PRECONDITIONER_LEARNED;
+  if (o.preconditioner != CGX_PRECONDITIONER_JACOBI && !want_learned)
     return fail(CGX_ERROR_UNSUPPORTED,
-                "mixed precision supports the Jacobi preconditioner");
+                "mixed precision supports the Jacobi and learned preconditioners");
   if (!h->c_valid)
     return fail(CGX_ERROR_INVALID_STATE, "Jacobi preconditioner not set");
+  if (want_learned && !(h->L && h->L->has_factor))
+    return fail(CGX_ERROR_INVALID_STATE,
+                "learned factor not set (cgx_learned_setup + cgx_learned_factor)");
   cudaStream_t s = h->stream;
   CUDA_TRY(cudaEventRecord(h->ev[6], s));
   CGX_TRY(ensure_f32(h));
 
-  GraphEntry *ge = nullptr;
+  auto outer_update = [&] {
+    k_outer_update<<<grid_stream(h, h->N), kThreads, 0, h->stream>>>(
+        h->N, h->vec[CGX_VECTOR_X], h->d32, h->st);
+    return cudaGetLastError();
+  };
+  auto guard = [&] {
+    k_loop_guard<<<1, 1, 0, h->stream>>>(h->st);
+    return cudaGetLastError();
+  };
+  GraphEntry *gj = nullptr, *gl = nullptr;
   if (o.loop == CGX_LOOP_GRAPH) {
     CGX_TRY(build_while_graph(
         h, 300,
@@ -1163,20 +1282,23 @@ static cgx_status solve_mixed(cgx_handle *h, const cgx_options &o,
         },
         [&] {
           cudaError_t e = launch_inner_iteration(h);
-          if (e != cudaSuccess) return e;
-          k_loop_guard<<<1, 1, 0, h->stream>>>(h->st);
-          return cudaGetLastError();
+          return e != cudaSuccess ? e : guard();
         },
-        [&] {
-          k_outer_update<<<grid_stream(h, h->N), kThreads, 0, h->stream>>>(
-              h->N, h->vec[CGX_VECTOR_X], h->d32, h->st);
-          return cudaGetLastError();
-        },
-        &ge));
+        outer_update, &gj));
+    if (want_learned)
+      CGX_TRY(build_while_graph(
+          h, 500, [&] { return launch_learned_start(h); },
+          [&] {
+            cudaError_t e = launch_learned_iteration(h);
+            return e != cudaSuccess ? e : guard();
+          },
+          outer_update, &gl));
   } else if (o.loop == CGX_LOOP_CHUNKED) {
     CGX_TRY(build_chunk_graph(h, 400, [&] { return launch_inner_iteration(h); },
-                              &ge));
+                              &gj));
   }
+  const unsigned long long cond_j = gj && o.loop == CGX_LOOP_GRAPH ? gj->cond : 0;
+  const unsigned long long cond_l = gl ? gl->cond : 0;
 
   // ||b||.
   double bnorm = 0;
@@ -1190,15 +1312,14 @@ static cgx_status solve_mixed(cgx_handle *h, const cgx_options &o,
     CUDA_TRY(cudaStreamSynchronize(s));
     bnorm = std::sqrt(h->host_scalar[0]);
   }
-  reset_host_state(h, o.max_iterations, o.tolerance,
-                   o.loop == CGX_LOOP_GRAPH, ge && o.loop == CGX_LOOP_GRAPH
-                                                 ? ge->cond
-                                                 : 0);
+  reset_host_state(h, o.max_iterations, o.tolerance, o.loop == CGX_LOOP_GRAPH,
+                   cond_j);
   h->host_st->bnorm = bnorm;
   h->host_st->inner_tol_min = o.inner_tolerance;
   CGX_TRY(push_state(h));
 
-  double rel = 0;
+  bool learned = want_learned;
+  double rel = 0, prev = -1;
   int outer = 0;
   double t_spmv = 0, t_upd = 0, t_dir = 0;
   int launches = 0;
@@ -1206,30 +1327,53 @@ static cgx_status solve_mixed(cgx_handle *h, const cgx_options &o,
     double r2;
     CGX_TRY(true_residual_r2(h, &r2));
     rel = bnorm > 0 ? std::sqrt(r2) / bnorm : std::sqrt(r2);
+    if (learned && outer > 0 && (!std::isfinite(rel) || rel > 0.5 * prev)) {
+      // The learned step failed: undo it and continue with Jacobi.
+      CUDA_TRY(cudaMemcpyAsync(h->vec[CGX_VECTOR_X], h->L->xbak,
+                               sizeof(double) * h->N, cudaMemcpyDeviceToDevice, s));
+      learned = false;
+      res.fell_back = 1;
+      CGX_TRY(true_residual_r2(h, &r2));
+      rel = bnorm > 0 ? std::sqrt(r2) / bnorm : std::sqrt(r2);
+    }
     if (!(rel > o.tolerance)) break;  // converged (or NaN: stop)
     if (outer >= o.max_outer) break;
     CGX_TRY(pull_state(h));
     if (h->host_st->total_inner >= o.max_iterations) break;
     outer++;
-    double tin = std::max(o.inner_tolerance, 0.5 * o.tolerance / rel);
-    // Inner tolerance and a fresh loop-guard count for this inner solve.
+    prev = rel;
+    if (learned)
+      CUDA_TRY(cudaMemcpyAsync(h->L->xbak, h->vec[CGX_VECTOR_X],
+                               sizeof(double) * h->N, cudaMemcpyDeviceToDevice, s));
+    const double tin = std::max(o.inner_tolerance, 0.5 * o.tolerance / rel);
+    // Inner tolerance, graph condition and a fresh loop-guard count.
     h->host_st->in_tol = tin;
     h->host_st->body_count = 0;
+    h->host_st->cond = learned ? cond_l : cond_j;
     CUDA_TRY(cudaMemcpyAsync(&h->st->in_tol, &h->host_st->in_tol,
                              sizeof(double), cudaMemcpyHostToDevice, s));
     CUDA_TRY(cudaMemcpyAsync(&h->st->body_count, &h->host_st->body_count,
                              sizeof(int), cudaMemcpyHostToDevice, s));
+    CUDA_TRY(cudaMemcpyAsync(&h->st->cond, &h->host_st->cond,
+                             sizeof(unsigned long long), cudaMemcpyHostToDevice, s));
     if (o.loop == CGX_LOOP_GRAPH) {
-      CUDA_TRY(cudaGraphLaunch(ge->exec, s));
+      CUDA_TRY(cudaGraphLaunch(learned ? gl->exec : gj->exec, s));
     } else {
-      k_inner_start<<<grid_stream(h, h->N), kThreads, 0, s>>>(
-          h->N, h->r64, h->r32, h->d32, h->p32, h->C32, h->st, h->partials,
-          ticket(h, kTicketInnerStart));
-      CUDA_TRY(cudaGetLastError());
+      if (learned) {
+        CUDA_TRY(launch_learned_start(h));
+      } else {
+        k_inner_start<<<grid_stream(h, h->N), kThreads, 0, s>>>(
+            h->N, h->r64, h->r32, h->d32, h->p32, h->C32, h->st, h->partials,
+            ticket(h, kTicketInnerStart));
+        CUDA_TRY(cudaGetLastError());
+      }
       const int maxLaunches = o.max_iterations + 2;
       for (int l = 0; l < maxLaunches; l++) {
-        if (o.loop == CGX_LOOP_CHUNKED) {
-          CUDA_TRY(cudaGraphLaunch(ge->exec, s));
+        if (learned) {
+          CUDA_TRY(launch_learned_iteration(
+              h, o.loop == CGX_LOOP_KERNELS ? h->ev : nullptr));
+        } else if (o.loop == CGX_LOOP_CHUNKED) {
+          CUDA_TRY(cudaGraphLaunch(gj->exec, s));
         } else {
           CUDA_TRY(launch_inner_iteration(h, h->ev));
         }
@@ -1248,9 +1392,7 @@ static cgx_status solve_mixed(cgx_handle *h, const cgx_options &o,
         }
         if (*(int *)h->host_scalar) break;
       }
-      k_outer_update<<<grid_stream(h, h->N), kThreads, 0, s>>>(
-          h->N, h->vec[CGX_VECTOR_X], h->d32, h->st);
-      CUDA_TRY(cudaGetLastError());
+      CUDA_TRY(outer_update());
     }
   }
   CUDA_TRY(cudaEventRecord(h->ev[7], s));
@@ -1270,6 +1412,487 @@ static cgx_status solve_mixed(cgx_handle *h, const cgx_options &o,
   res.spmv_launches = res.update_launches = res.direction_launches = launches;
   return CGX_SUCCESS;
 }
+
+// ---------------------------------------------------------------------------
+// Learned preconditioner
+
+namespace {
+
+using namespace cgx::learned;
+
+template <typename T>
+size_t take_n(Carver &c, size_t n) {
+  return c.take<T>(n + kPad);
+}
+
+int grid_for(const cgx_handle *h, size_t work) { return grid_stream(h, work); }
+
+// Exclusive scan of in[0..n) into out[0..n] (out[n] = total).
+cudaError_t scan(cgx_handle *h, int n, const int *in, int *out, int *sums) {
+  const int nb = (n + kScanBlock - 1) / kScanBlock;
+  k_scan_blocks<<<nb, kScanBlock, 0, h->stream>>>(n, in, out, sums);
+  k_scan_sums<<<1, kScanBlock, 0, h->stream>>>(nb, sums);
+  k_scan_add<<<nb, kScanBlock, 0, h->stream>>>(n, out, sums);
+  return cudaGetLastError();
+}
+
+cgx_status learned_alloc(cgx_handle *h, int nnzL) {
+  Learned *L = h->L;
+  const int N = h->N;
+  Carver c;
+  size_t o_dis = take_n<double>(c, N), o_ahat = take_n<float>(c, h->nz);
+  size_t o_feat = take_n<float>(c, (size_t)N * NIN);
+  size_t o_nlow = take_n<int>(c, N), o_nup = take_n<int>(c, N);
+  size_t o_sums = take_n<int>(c, L->nblocks), o_flag = take_n<int>(c, 4);
+  size_t o_gptr = take_n<int>(c, N + 1), o_tptr = take_n<int>(c, N + 1);
+  size_t o_gcol = take_n<int>(c, nnzL), o_grow = take_n<int>(c, nnzL);
+  size_t o_g2a = take_n<int>(c, nnzL), o_tcol = take_n<int>(c, nnzL);
+  size_t o_t2g = take_n<int>(c, nnzL), o_g2t = take_n<int>(c, nnzL);
+  size_t o_ghat = take_n<float>(c, nnzL), o_gs = take_n<float>(c, nnzL);
+  size_t o_gts = take_n<float>(c, nnzL);
+  size_t o_h[4], o_agg[3], o_pre[4];
+  for (int k = 0; k < 4; k++) o_h[k] = take_n<__nv_bfloat16>(c, (size_t)N * W);
+  for (int k = 0; k < 3; k++) o_agg[k] = take_n<__nv_bfloat16>(c, (size_t)N * W);
+  for (int k = 0; k < 4; k++) o_pre[k] = take_n<float>(c, (size_t)N * W);
+  size_t o_o = take_n<float>(c, (size_t)N * NOUT);
+  size_t o_y = take_n<float>(c, N), o_z = take_n<float>(c, N);
+  size_t o_xb = take_n<double>(c, N);
+  CUDA_TRY(cudaMalloc(&L->mem, c.off));
+  CUDA_TRY(cudaMemsetAsync(L->mem, 0, c.off, h->stream));
+  char *b = (char *)L->mem;
+  L->dis = (double *)(b + o_dis);
+  L->ahat = (float *)(b + o_ahat);
+  L->feat = (float *)(b + o_feat);
+  L->nlow = (int *)(b + o_nlow);
+  L->nup = (int *)(b + o_nup);
+  L->sums = (int *)(b + o_sums);
+  L->flag = (int *)(b + o_flag);
+  L->gptr = (int *)(b + o_gptr);
+  L->tptr = (int *)(b + o_tptr);
+  L->gcol = (int *)(b + o_gcol);
+  L->grow = (int *)(b + o_grow);
+  L->g2a = (int *)(b + o_g2a);
+  L->tcol = (int *)(b + o_tcol);
+  L->t2g = (int *)(b + o_t2g);
+  L->g2t = (int *)(b + o_g2t);
+  L->ghat = (float *)(b + o_ghat);
+  L->gs = (float *)(b + o_gs);
+  L->gts = (float *)(b + o_gts);
+  for (int k = 0; k < 4; k++) L->h[k] = (__nv_bfloat16 *)(b + o_h[k]);
+  for (int k = 0; k < 3; k++) L->agg[k] = (__nv_bfloat16 *)(b + o_agg[k]);
+  for (int k = 0; k < 4; k++) L->pre[k] = (float *)(b + o_pre[k]);
+  L->o = (float *)(b + o_o);
+  L->y32 = (float *)(b + o_y);
+  L->z32 = (float *)(b + o_z);
+  L->xbak = (double *)(b + o_xb);
+  return CGX_SUCCESS;
+}
+
+cgx_status learned_train_alloc(cgx_handle *h) {
+  Learned *L = h->L;
+  if (L->train) return CGX_SUCCESS;
+  const int N = h->N;
+  Carver c;
+  size_t o[20];
+  int k = 0;
+  for (int q = 0; q < 6; q++) o[k++] = take_n<float>(c, (size_t)N * S);
+  o[k++] = take_n<float>(c, L->nnzL);                 // dg
+  o[k++] = take_n<float>(c, (size_t)N * NOUT);        // dO
+  for (int q = 0; q < 5; q++) o[k++] = take_n<float>(c, (size_t)N * W);
+  o[k++] = take_n<float>(c, (size_t)kMaxGrid * (W * 2 * W + W));  // partial
+  o[k++] = take_n<float>(c, NPARAMS);                 // grad
+  o[k++] = take_n<float>(c, 4);                       // loss
+  o[k++] = take_n<float>(c, 2 * (W * W + W));         // gtmp
+  CUDA_TRY(cudaMalloc(&L->train, c.off));
+  CUDA_TRY(cudaMemsetAsync(L->train, 0, c.off, h->stream));
+  char *b = (char *)L->train;
+  k = 0;
+  L->V = (float *)(b + o[k++]);
+  L->T1 = (float *)(b + o[k++]);
+  L->T2 = (float *)(b + o[k++]);
+  L->rho = (float *)(b + o[k++]);
+  L->dT2 = (float *)(b + o[k++]);
+  L->dT1 = (float *)(b + o[k++]);
+  L->dg = (float *)(b + o[k++]);
+  L->dO = (float *)(b + o[k++]);
+  L->dh = (float *)(b + o[k++]);
+  L->dh2 = (float *)(b + o[k++]);
+  L->dself = (float *)(b + o[k++]);
+  L->dagg = (float *)(b + o[k++]);
+  L->dpre = (float *)(b + o[k++]);
+  L->partial = (float *)(b + o[k++]);
+  L->grad = (float *)(b + o[k++]);
+  L->loss = (float *)(b + o[k++]);
+  L->gtmp = (float *)(b + o[k++]);
+  return CGX_SUCCESS;
+}
+
+// Forward pass of the network on h's scaled graph; writes Ghat (and the
+// scaled G, G^T for the apply when `scaled`).
+cudaError_t gnn_forward(cgx_handle *h, const float *P, bool scaled) {
+  Learned *L = h->L;
+  const int N = h->N;
+  cudaStream_t s = h->stream;
+  k_embed<<<grid_for(h, (size_t)N * W), kThreads, 0, s>>>(N, L->feat, P, L->h[0],
+                                                          L->pre[0]);
+  const int groups = (N + 15) / 16;
+  const int lgrid = std::max(
+      1, std::min(h->num_sms * 8, (groups + kLayerWarps - 1) / kLayerWarps));
+  for (int l = 0; l < 3; l++)
+    k_layer<<<lgrid, 32 * kLayerWarps, 0, s>>>(N, h->ptr, h->index, L->ahat, P,
+                                               l, L->h[l], L->h[l + 1],
+                                               L->agg[l], L->pre[l + 1]);
+  k_head<<<grid_for(h, (size_t)N * NOUT), kThreads, 0, s>>>(N, L->h[3], P, L->o);
+  k_assemble<<<grid_for(h, L->nnzL), kThreads, 0, s>>>(
+      L->nnzL, L->grow, L->gcol, L->g2a, L->ahat, L->o, L->ghat, L->dis,
+      L->g2t, scaled ? L->gs : nullptr, scaled ? L->gts : nullptr);
+  return cudaGetLastError();
+}
+
+// Loss and gradient (into L->grad) for the probes in L->V.
+cudaError_t gnn_backward(cgx_handle *h, const float *P) {
+  Learned *L = h->L;
+  const int N = h->N;
+  cudaStream_t s = h->stream;
+  const int g = grid_for(h, N);
+  // T1 = Ghat V, T2 = Ahat T1, R = Ghat^T T2 - V.
+  k_spmm8<<<g, kThreads, 0, s>>>(N, L->gptr, L->gcol, L->ghat, nullptr, L->V, L->T1);
+  k_spmm8<<<g, kThreads, 0, s>>>(N, h->ptr, h->index, L->ahat, nullptr, L->T1, L->T2);
+  k_loss_residual<<<g, kThreads, 0, s>>>(N, L->tptr, L->tcol, L->ghat, L->t2g,
+                                         L->T2, L->V, L->rho, h->partials,
+                                         ticket(h, kTicketDot), L->loss);
+  // dT2 = Ghat rho, dT1 = Ahat dT2, dGhat.
+  k_spmm8<<<g, kThreads, 0, s>>>(N, L->gptr, L->gcol, L->ghat, nullptr, L->rho, L->dT2);
+  k_spmm8<<<g, kThreads, 0, s>>>(N, h->ptr, h->index, L->ahat, nullptr, L->dT2, L->dT1);
+  k_grad_factor<<<g, kThreads, 0, s>>>(N, L->gptr, L->gcol, L->T2, L->dT1, L->rho,
+                                       L->V, L->dg);
+  k_grad_head_out<<<g, kThreads, 0, s>>>(N, L->gptr, L->gcol, L->g2a, L->tptr,
+                                         L->tcol, L->t2g, L->ahat, L->o, L->dg,
+                                         L->dO);
+  const int pg = std::max(1, std::min(kMaxGrid, (N + 31) / 32));
+  // Head weights: dW_h = sum dO h3^T, db_h = sum dO.
+  k_outer_partials<NOUT, W, __nv_bfloat16><<<pg, kThreads, 0, s>>>(
+      N, L->dO, L->h[3], L->partial);
+  k_reduce_partials<<<grid_for(h, NOUT * W + NOUT), kThreads, 0, s>>>(
+      pg, NOUT * W + NOUT, L->partial, L->grad + OFF_WH);
+  k_grad_head_in<<<grid_for(h, (size_t)N * W), kThreads, 0, s>>>(N, P, L->dO, L->dh);
+  // Layers 2..0.
+  float *dcur = L->dh, *dnext = L->dh2;
+  for (int l = 2; l >= 0; l--) {
+    k_layer_back1<<<grid_for(h, (size_t)N * W), kThreads, 0, s>>>(
+        N, P, l, dcur, L->pre[l + 1], L->dpre, L->dself, L->dagg);
+    // dW_l[:, 0:W] = sum dpre h_l^T (+ bias), dW_l[:, W:2W] = sum dpre agg^T.
+    k_outer_partials<W, W, __nv_bfloat16><<<pg, kThreads, 0, s>>>(
+        N, L->dpre, L->h[l], L->partial);
+    k_reduce_partials<<<grid_for(h, W * W + W), kThreads, 0, s>>>(
+        pg, W * W + W, L->partial, L->gtmp);
+    k_outer_partials<W, W, __nv_bfloat16><<<pg, kThreads, 0, s>>>(
+        N, L->dpre, L->agg[l], L->partial);
+    k_reduce_partials<<<grid_for(h, W * W + W), kThreads, 0, s>>>(
+        pg, W * W + W, L->partial, L->gtmp + (W * W + W));
+    k_pack_layer_grad<<<1, kThreads, 0, s>>>(L->gtmp, L->grad + OFF_L0 + l * L_STRIDE);
+    k_layer_back2<<<grid_for(h, (size_t)N * 32), kThreads, 0, s>>>(
+        N, h->ptr, h->index, L->ahat, L->dself, L->dagg, dnext);
+    std::swap(dcur, dnext);
+  }
+  // Embedding.
+  k_relu_back<<<grid_for(h, (size_t)N * W), kThreads, 0, s>>>(N * W, L->pre[0], dcur);
+  k_outer_partials<W, NIN, float><<<pg, kThreads, 0, s>>>(N, dcur, L->feat,
+                                                          L->partial);
+  k_reduce_partials<<<grid_for(h, W * NIN + W), kThreads, 0, s>>>(
+      pg, W * NIN + W, L->partial, L->grad + OFF_WIN);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+extern "C" {
+
+int cgx_gnn_param_count(void) { return NPARAMS; }
+
+cgx_status cgx_gnn_create(cgx_gnn **out, int device, const float *params) {
+  if (!out) return fail(CGX_ERROR_INVALID_ARGUMENT, "out is NULL");
+  *out = nullptr;
+  int n = 0;
+  cgx_device_count(&n);
+  if (device < 0 || device >= n)
+    return fail(CGX_ERROR_INVALID_ARGUMENT, "no CUDA device " + std::to_string(device));
+  DeviceGuard guard(device);
+  cgx_gnn *g = new cgx_gnn();
+  g->device = device;
+  cudaError_t e = cudaMalloc(&g->params, sizeof(float) * 3 * NPARAMS);
+  if (e != cudaSuccess) {
+    delete g;
+    return cuda_fail(e, "cudaMalloc (network parameters)");
+  }
+  g->m = g->params + NPARAMS;
+  g->v = g->params + 2 * NPARAMS;
+  e = cudaMemset(g->params, 0, sizeof(float) * 3 * NPARAMS);
+  if (e == cudaSuccess && params)
+    e = cudaMemcpy(g->params, params, sizeof(float) * NPARAMS,
+                   cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    cudaFree(g->params);
+    delete g;
+    return cuda_fail(e, "network parameter upload");
+  }
+  *out = g;
+  return CGX_SUCCESS;
+}
+
+cgx_status cgx_gnn_destroy(cgx_gnn *g) {
+  if (!g) return CGX_SUCCESS;
+  DeviceGuard guard(g->device);
+  cudaFree(g->params);
+  delete g;
+  return CGX_SUCCESS;
+}
+
+cgx_status cgx_gnn_set_params(cgx_gnn *g, const float *params) {
+  if (!g || !params) return fail(CGX_ERROR_INVALID_ARGUMENT, "NULL argument");
+  DeviceGuard guard(g->device);
+  CUDA_TRY(cudaMemcpy(g->params, params, sizeof(float) * NPARAMS,
+                      cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemset(g->m, 0, sizeof(float) * 2 * NPARAMS));
+  g->step = 0;
+  return CGX_SUCCESS;
+}
+
+cgx_status cgx_gnn_get_params(cgx_gnn *g, float *params) {
+  if (!g || !params) return fail(CGX_ERROR_INVALID_ARGUMENT, "NULL argument");
+  DeviceGuard guard(g->device);
+  CUDA_TRY(cudaMemcpy(params, g->params, sizeof(float) * NPARAMS,
+                      cudaMemcpyDeviceToHost));
+  return CGX_SUCCESS;
+}
+
+cgx_status cgx_update_crs_values(cgx_handle *h, const double *value) {
+  CGX_TRY(need_matrix(h));
+  if (h->format != CGX_FORMAT_CRS)
+    return fail(CGX_ERROR_INVALID_STATE, "the uploaded matrix is not CRS");
+  if (!value && h->nz > 0) return fail(CGX_ERROR_INVALID_ARGUMENT, "value is NULL");
+  DeviceGuard guard(h->device);
+  if (h->nz > 0)
+    CUDA_TRY(cudaMemcpyAsync(h->value, value, sizeof(double) * h->nz,
+                             cudaMemcpyDefault, h->stream));
+  h->f32_valid = false;
+  h->c_valid = false;
+  if (h->L) h->L->has_factor = false;
+  return CGX_SUCCESS;
+}
+
+cgx_status cgx_learned_setup(cgx_handle *h) {
+  CGX_TRY(need_matrix(h));
+  if (h->format != CGX_FORMAT_CRS)
+    return fail(CGX_ERROR_UNSUPPORTED, "the learned preconditioner needs CRS");
+  DeviceGuard guard(h->device);
+  cudaStream_t s = h->stream;
+  const int N = h->N;
+  const bool fresh = !h->L;
+  if (fresh) {
+    h->L = new Learned();
+    h->L->N = N;
+    h->L->nnz = h->nz;
+    h->L->nblocks = (N + kScanBlock - 1) / kScanBlock;
+  }
+  Learned *L = h->L;
+  // Pass 1: scaling, features, counts (needs a temporary flag and counts;
+  // on a fresh set-up the buffers are sized after the counts are known).
+  int *flag = nullptr, *nlow = nullptr, *nup = nullptr;
+  double *dis = nullptr;
+  float *ahat = nullptr, *feat = nullptr;
+  void *tmp = nullptr;
+  if (fresh) {
+    Carver c;
+    size_t o_dis = c.take<double>(N + kPad), o_ahat = c.take<float>(h->nz + kPad);
+    size_t o_feat = c.take<float>((size_t)N * NIN + kPad);
+    size_t o_nl = c.take<int>(N + kPad), o_nu = c.take<int>(N + kPad);
+    size_t o_f = c.take<int>(4);
+    CUDA_TRY(cudaMalloc(&tmp, c.off));
+    char *b = (char *)tmp;
+    dis = (double *)(b + o_dis);
+    ahat = (float *)(b + o_ahat);
+    feat = (float *)(b + o_feat);
+    nlow = (int *)(b + o_nl);
+    nup = (int *)(b + o_nu);
+    flag = (int *)(b + o_f);
+  } else {
+    dis = L->dis; ahat = L->ahat; feat = L->feat;
+    nlow = L->nlow; nup = L->nup; flag = L->flag;
+  }
+  CUDA_TRY(cudaMemsetAsync(flag, 0, sizeof(int), s));
+  const int g = grid_stream(h, N);
+  k_inv_sqrt_diag<<<g, kThreads, 0, s>>>(N, h->ptr, h->index, h->value, dis, flag);
+  k_scaled_rows<<<g, kThreads, 0, s>>>(N, h->ptr, h->index, h->value, dis, ahat,
+                                       feat, nlow, nup);
+  CUDA_TRY(cudaGetLastError());
+  if (!fresh) {
+    CUDA_TRY(cudaMemcpyAsync(h->host_scalar, flag, sizeof(int),
+                             cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    if (*(int *)h->host_scalar)
+      return fail(CGX_ERROR_UNSUPPORTED,
+                  "learned preconditioner: a diagonal entry is missing or not positive");
+    L->has_factor = false;
+    return CGX_SUCCESS;  // pattern unchanged (cgx_update_crs_values)
+  }
+  // Lower/upper totals.
+  {
+    // Scan lower counts into a temporary ptr to learn nnzL.
+    int nb = L->nblocks;
+    int *tptr_tmp = nullptr, *sums_tmp = nullptr;
+    Carver c;
+    size_t o_p = c.take<int>(N + 1 + kPad), o_s = c.take<int>(nb + kPad);
+    void *t2 = nullptr;
+    CUDA_TRY(cudaMalloc(&t2, c.off));
+    tptr_tmp = (int *)((char *)t2 + o_p);
+    sums_tmp = (int *)((char *)t2 + o_s);
+    CUDA_TRY(scan(h, N, nlow, tptr_tmp, sums_tmp));
+    int totals[2] = {0, 0};
+    CUDA_TRY(cudaMemcpyAsync(&totals[0], tptr_tmp + N, sizeof(int),
+                             cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(scan(h, N, nup, tptr_tmp, sums_tmp));
+    CUDA_TRY(cudaMemcpyAsync(&totals[1], tptr_tmp + N, sizeof(int),
+                             cudaMemcpyDeviceToHost, s));
+    int fl = 0;
+    CUDA_TRY(cudaMemcpyAsync(&fl, flag, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    cudaFree(t2);
+    if (fl) {
+      cudaFree(tmp);
+      free_learned(h);
+      return fail(CGX_ERROR_UNSUPPORTED,
+                  "learned preconditioner: a diagonal entry is missing or not positive");
+    }
+    if (totals[0] != totals[1]) {
+      cudaFree(tmp);
+      free_learned(h);
+      return fail(CGX_ERROR_UNSUPPORTED,
+                  "learned preconditioner: the matrix pattern is not symmetric");
+    }
+    L->nnzL = totals[0];
+  }
+  cgx_status st = learned_alloc(h, L->nnzL);
+  if (st != CGX_SUCCESS) {
+    cudaFree(tmp);
+    free_learned(h);
+    return st;
+  }
+  // Move pass-1 results into place, build the patterns and maps.
+  CUDA_TRY(cudaMemcpyAsync(L->dis, dis, sizeof(double) * N, cudaMemcpyDeviceToDevice, s));
+  CUDA_TRY(cudaMemcpyAsync(L->ahat, ahat, sizeof(float) * h->nz, cudaMemcpyDeviceToDevice, s));
+  CUDA_TRY(cudaMemcpyAsync(L->feat, feat, sizeof(float) * N * NIN, cudaMemcpyDeviceToDevice, s));
+  CUDA_TRY(cudaMemcpyAsync(L->nlow, nlow, sizeof(int) * N, cudaMemcpyDeviceToDevice, s));
+  CUDA_TRY(cudaMemcpyAsync(L->nup, nup, sizeof(int) * N, cudaMemcpyDeviceToDevice, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  cudaFree(tmp);
+  CUDA_TRY(scan(h, N, L->nlow, L->gptr, L->sums));
+  CUDA_TRY(scan(h, N, L->nup, L->tptr, L->sums));
+  k_fill_patterns<<<g, kThreads, 0, s>>>(N, h->ptr, h->index, L->gptr, L->tptr,
+                                         L->gcol, L->grow, L->tcol, L->g2a);
+  CUDA_TRY(cudaMemsetAsync(L->flag, 0, sizeof(int), s));
+  k_transpose_map<<<grid_stream(h, L->nnzL), kThreads, 0, s>>>(
+      L->nnzL, L->grow, L->gcol, L->tptr, L->tcol, L->g2t, L->t2g, L->flag);
+  CUDA_TRY(cudaGetLastError());
+  CUDA_TRY(cudaMemcpyAsync(h->host_scalar, L->flag, sizeof(int),
+                           cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  if (*(int *)h->host_scalar) {
+    free_learned(h);
+    return fail(CGX_ERROR_UNSUPPORTED,
+                "learned preconditioner: the matrix pattern is not symmetric");
+  }
+  drop_graphs(h);  // graphs that use the learned buffers are rebuilt
+  return CGX_SUCCESS;
+}
+
+cgx_status cgx_learned_factor(cgx_handle *h, cgx_gnn *gn, double eps) {
+  CGX_TRY(need_matrix(h));
+  if (!gn) return fail(CGX_ERROR_INVALID_ARGUMENT, "network is NULL");
+  if (!h->L) return fail(CGX_ERROR_INVALID_STATE, "call cgx_learned_setup first");
+  if (gn->device != h->device)
+    return fail(CGX_ERROR_INVALID_ARGUMENT, "network and handle on different devices");
+  if (!(eps >= 0)) return fail(CGX_ERROR_INVALID_ARGUMENT, "eps must be >= 0");
+  DeviceGuard guard(h->device);
+  CUDA_TRY(gnn_forward(h, gn->params, true));
+  h->L->eps = (float)eps;
+  h->L->has_factor = true;
+  return CGX_SUCCESS;
+}
+
+cgx_status cgx_learned_get_factor(cgx_handle *h, int *nnzL, float *ghat,
+                                  int *rows, int *cols) {
+  CGX_TRY(need_matrix(h));
+  if (!h->L) return fail(CGX_ERROR_INVALID_STATE, "call cgx_learned_setup first");
+  DeviceGuard guard(h->device);
+  Learned *L = h->L;
+  if (nnzL) *nnzL = L->nnzL;
+  if (ghat)
+    CUDA_TRY(cudaMemcpyAsync(ghat, L->ghat, sizeof(float) * L->nnzL,
+                             cudaMemcpyDeviceToHost, h->stream));
+  if (rows)
+    CUDA_TRY(cudaMemcpyAsync(rows, L->grow, sizeof(int) * L->nnzL,
+                             cudaMemcpyDeviceToHost, h->stream));
+  if (cols)
+    CUDA_TRY(cudaMemcpyAsync(cols, L->gcol, sizeof(int) * L->nnzL,
+                             cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return CGX_SUCCESS;
+}
+
+cgx_status cgx_gnn_loss_grad(cgx_gnn *gn, cgx_handle *h, const float *probes,
+                             unsigned long long seed, float *loss, float *grad) {
+  CGX_TRY(need_matrix(h));
+  if (!gn) return fail(CGX_ERROR_INVALID_ARGUMENT, "network is NULL");
+  if (!h->L) return fail(CGX_ERROR_INVALID_STATE, "call cgx_learned_setup first");
+  DeviceGuard guard(h->device);
+  CGX_TRY(learned_train_alloc(h));
+  Learned *L = h->L;
+  cudaStream_t s = h->stream;
+  if (probes)
+    CUDA_TRY(cudaMemcpyAsync(L->V, probes, sizeof(float) * h->N * S,
+                             cudaMemcpyHostToDevice, s));
+  else
+    k_rademacher<<<grid_stream(h, (size_t)h->N * S), kThreads, 0, s>>>(h->N, seed, L->V);
+  CUDA_TRY(gnn_forward(h, gn->params, false));
+  CUDA_TRY(gnn_backward(h, gn->params));
+  if (loss)
+    CUDA_TRY(cudaMemcpyAsync(loss, L->loss, sizeof(float), cudaMemcpyDeviceToHost, s));
+  if (grad)
+    CUDA_TRY(cudaMemcpyAsync(grad, L->grad, sizeof(float) * NPARAMS,
+                             cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  L->has_factor = false;  // the factor buffers now hold unscaled values
+  return CGX_SUCCESS;
+}
+
+cgx_status cgx_gnn_train_step(cgx_gnn *gn, cgx_handle *h, unsigned long long seed,
+                              float lr, float *loss) {
+  CGX_TRY(need_matrix(h));
+  if (!gn) return fail(CGX_ERROR_INVALID_ARGUMENT, "network is NULL");
+  if (!h->L) return fail(CGX_ERROR_INVALID_STATE, "call cgx_learned_setup first");
+  if (!(lr > 0)) return fail(CGX_ERROR_INVALID_ARGUMENT, "lr must be > 0");
+  DeviceGuard guard(h->device);
+  CGX_TRY(learned_train_alloc(h));
+  Learned *L = h->L;
+  cudaStream_t s = h->stream;
+  k_rademacher<<<grid_stream(h, (size_t)h->N * S), kThreads, 0, s>>>(h->N, seed, L->V);
+  CUDA_TRY(gnn_forward(h, gn->params, false));
+  CUDA_TRY(gnn_backward(h, gn->params));
+  gn->step++;
+  k_adam<<<(NPARAMS + kThreads - 1) / kThreads, kThreads, 0, s>>>(
+      NPARAMS, gn->params, gn->m, gn->v, L->grad, lr, 0.9f, 0.999f, 1e-8f, gn->step);
+  CUDA_TRY(cudaGetLastError());
+  if (loss) {
+    CUDA_TRY(cudaMemcpyAsync(loss, L->loss, sizeof(float), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+  }
+  L->has_factor = false;
+  return CGX_SUCCESS;
+}
+
+}  // extern "C"
+
 
 extern "C" {
 
@@ -1308,9 +1931,10 @@ cgx_status cgx_solve(cgx_handle *h, const cgx_options *opts,
       o.precision < CGX_PRECISION_FP64 || o.precision > CGX_PRECISION_MIXED ||
       o.loop < CGX_LOOP_GRAPH || o.loop > CGX_LOOP_KERNELS)
     return fail(CGX_ERROR_INVALID_ARGUMENT, "invalid option value");
-  if (o.preconditioner == CGX_PRECONDITIONER_LEARNED)
+  if (o.preconditioner == CGX_PRECONDITIONER_LEARNED &&
+      o.precision != CGX_PRECISION_MIXED)
     return fail(CGX_ERROR_UNSUPPORTED,
-                "learned preconditioner: use cgx_solve_learned");
+                "the learned preconditioner runs in the mixed-precision solve");
   if (o.precision == CGX_PRECISION_MIXED && !(o.inner_tolerance > 0))
     return fail(CGX_ERROR_INVALID_ARGUMENT, "inner_tolerance must be > 0");
   DeviceGuard guard(h->device);

@@ -58,6 +58,61 @@ __host__ __device__ inline size_t align16(size_t b) {
   return (b + 15) & ~(size_t)15;
 }
 
+// Sum of row entries [j0, j1) in storage order: value(j) * x[col(j)]. The
+// loads of a group of 8 entries are all issued before the first multiply-add,
+// so up to 8 gathers of x are in flight per thread; the additions still run
+// one after another in entry order, so the FP64 result is unchanged.
+template <typename VT, int U = 8, typename ValF, typename ColF>
+__device__ __forceinline__ VT row_sum(int j0, int j1, ValF val, ColF col,
+                                      const VT *__restrict__ x) {
+  VT sum = 0;
+  for (int j = j0; j < j1; j += U) {
+    VT v[U], xv[U];
+#pragma unroll
+    for (int k = 0; k < U; k++) {
+      if (j + k < j1) {
+        v[k] = val(j + k);
+        xv[k] = __ldg(&x[col(j + k)]);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < U; k++)
+      if (j + k < j1) sum = madd(sum, v[k], xv[k]);
+  }
+  return sum;
+}
+
+// Row sum from shared-memory staged values/indices: the U gathers of x of a
+// group are issued first (only they occupy registers); the values are read
+// from shared memory just before each multiply-add, in entry order.
+template <typename VT, int U>
+__device__ __forceinline__ VT row_sum_staged(int j0, int j1,
+                                             const VT *__restrict__ sv,
+                                             const int *__restrict__ si,
+                                             const VT *__restrict__ x) {
+  VT sum = 0;
+  for (int j = j0; j < j1; j += U) {
+    VT xv[U];
+#pragma unroll
+    for (int k = 0; k < U; k++)
+      if (j + k < j1) xv[k] = __ldg(&x[si[j + k]]);
+#pragma unroll
+    for (int k = 0; k < U; k++)
+      if (j + k < j1) sum = madd(sum, sv[j + k], xv[k]);
+  }
+  return sum;
+}
+
+// Plain sequential row sum (rare paths where ILP does not matter).
+template <typename VT, typename ValF, typename ColF>
+__device__ __forceinline__ VT row_sum_serial(int j0, int j1, ValF val,
+                                             ColF col,
+                                             const VT *__restrict__ x) {
+  VT sum = 0;
+  for (int j = j0; j < j1; j++) sum = madd(sum, val(j), __ldg(&x[col(j)]));
+  return sum;
+}
+
 // Dynamic shared memory of the staged CRS kernel for a given tile capacity.
 template <typename VT>
 __host__ __device__ inline size_t crs_stage_bytes(int cap) {
@@ -142,11 +197,12 @@ __global__ void __launch_bounds__(kThreads)
         if (ok) {
           const VT *sv = (buf ? sval1 : sval0) - (s & ~(VPER - 1));
           const int *si = (buf ? sidx1 : sidx0) - (s & ~3);
-          for (int j = j0; j < j1; j++) sum = madd(sum, sv[j], __ldg(&x[si[j]]));
+          sum = row_sum_staged<VT, 8>(j0, j1, sv, si, x);
         }
       } else {
-        for (int j = j0; j < j1; j++)
-          sum = madd(sum, __ldg(&A.value[j]), __ldg(&x[__ldg(&A.index[j])]));
+        sum = row_sum_serial<VT>(
+            j0, j1, [&](int j) { return __ldg(&A.value[j]); },
+            [&](int j) { return __ldg(&A.index[j]); }, x);
       }
       op.row(row, sum, acc);
     }
@@ -171,10 +227,12 @@ __global__ void __launch_bounds__(kThreads)
   for (int row = blockIdx.x * kThreads + threadIdx.x; row < N;
        row += gridDim.x * kThreads) {
     const int len = __ldg(&A.length[row]);
-    VT sum = 0;
-    size_t k = (size_t)row;
-    for (int j = 0; j < len; j++, k += (size_t)N)
-      sum = madd(sum, __ldg(&A.data[k]), __ldg(&x[__ldg(&A.index[k])]));
+    const VT *dat = A.data + row;
+    const int *idx = A.index + row;
+    const size_t n = (size_t)N;
+    const VT sum = row_sum<VT, 4>(
+        0, len, [&](int j) { return __ldg(&dat[(size_t)j * n]); },
+        [&](int j) { return __ldg(&idx[(size_t)j * n]); }, x);
     op.row(row, sum, acc);
   }
   op.finish(acc, st, partials);
@@ -206,11 +264,9 @@ __global__ void __launch_bounds__(kThreads)
   for (int row = blockIdx.x * kThreads + threadIdx.x; row < A.N;
        row += gridDim.x * kThreads) {
     const int j0 = __ldg(&A.rowStart[row]), j1 = __ldg(&A.rowStart[row + 1]);
-    double sum = 0;
-    for (int j = j0; j < j1; j++) {
-      const int e = __ldg(&A.perm[j]);
-      sum = madd(sum, __ldg(&A.V[e]), __ldg(&x[__ldg(&A.J[e])]));
-    }
+    const double sum = row_sum<double>(
+        j0, j1, [&](int j) { return __ldg(&A.V[__ldg(&A.perm[j])]); },
+        [&](int j) { return __ldg(&A.J[__ldg(&A.perm[j])]); }, x);
     op.row(row, sum, acc);
   }
   op.finish(acc, st, partials);
@@ -652,6 +708,118 @@ __global__ void __launch_bounds__(kThreads)
     const float pv = p[i];
     d[i] = fmaf(a, pv, d[i]);
     if (upd) p[i] = fmaf(b, pv, C[i] * r[i]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Inner FP32 PCG with an explicit preconditioned residual z = M^-1 r (the
+// learned factor: z = G (G^T r) + eps C r, two SpMVs with a global
+// dependency between them, so z is stored).
+
+// Start: r32 = r64 / ||r64||, d = 0, ||r32||; the first z and p = z come from
+// the apply that follows (OpLearnedZ in start mode).
+__global__ void __launch_bounds__(kThreads)
+    k_inner_start_z(int N, const double *__restrict__ r64,
+                    float *__restrict__ r, float *__restrict__ d, CgState *st,
+                    double *partials, unsigned *ticket) {
+  const double inv = 1.0 / sqrt(st->r2);
+  double rr = 0.0;
+  for (int i = blockIdx.x * kThreads + threadIdx.x; i < N;
+       i += gridDim.x * kThreads) {
+    const float ri = (float)(r64[i] * inv);
+    r[i] = ri;
+    d[i] = 0.0f;
+    rr = fma((double)ri, (double)ri, rr);
+  }
+  double in[1] = {rr}, out[1];
+  if (grid_reduce<1>(in, partials, ticket, out) && threadIdx.x == 0) {
+    st->in_nrm0 = sqrt(out[0]);
+    st->in_iter = 0;
+    st->in_stop = 0;
+    st->in_finished = 0;
+    if (st->use_cond)
+      cudaGraphSetConditional((cudaGraphConditionalHandle)st->cond, 1u);
+  }
+}
+
+// y = M r for the first factor of the apply; skipped once the loop stopped.
+struct OpInnerStore {
+  using Acc = NoAcc;
+  float *y;
+  __device__ bool skip(const CgState *st) const { return st->in_stop != 0; }
+  __device__ void row(int i, float s, Acc &) const { y[i] = s; }
+  __device__ void finish(Acc &, CgState *, double *) const {}
+};
+
+// z = s + eps C r (s = row of G y), <r,z>; in start mode also p = z and
+// rho = <r,z>, otherwise b = <r,z> / rho_old.
+struct OpLearnedZ {
+  using Acc = Acc1;
+  const float *r, *C;
+  float *z, *p;
+  float eps;
+  int start;
+  unsigned *ticket;
+  __device__ bool skip(const CgState *st) const { return st->in_stop != 0; }
+  __device__ void row(int i, float s, Acc &a) const {
+    const float ri = __ldg(&r[i]);
+    const float zi = fmaf(eps * __ldg(&C[i]), ri, s);
+    z[i] = zi;
+    if (start) p[i] = zi;
+    a.a0 = fma((double)ri, (double)zi, a.a0);
+  }
+  __device__ void finish(Acc &a, CgState *st, double *partials) const {
+    double in[1] = {a.a0}, out[1];
+    if (grid_reduce<1>(in, partials, ticket, out) && threadIdx.x == 0) {
+      if (start) {
+        st->in_rho = out[0];
+      } else {
+        st->in_beta = out[0] / st->in_rho;
+        st->in_rho = out[0];
+      }
+    }
+  }
+};
+
+// r -= a q; <r,r>; residual test (z and b follow from the apply).
+__global__ void __launch_bounds__(kThreads)
+    k_inner_update_z(int N, float *__restrict__ r, const float *__restrict__ q,
+                     CgState *st, double *partials, unsigned *ticket) {
+  if (st->in_stop) return;
+  const float na = (float)(-st->in_alpha);
+  double rr = 0.0;
+  for (int i = blockIdx.x * kThreads + threadIdx.x; i < N;
+       i += gridDim.x * kThreads) {
+    const float ri = fmaf(na, q[i], r[i]);
+    r[i] = ri;
+    rr = fma((double)ri, (double)ri, rr);
+  }
+  double in[1] = {rr}, out[1];
+  if (grid_reduce<1>(in, partials, ticket, out) && threadIdx.x == 0) {
+    st->in_iter += 1;
+    st->total_inner += 1;
+    const double res = sqrt(out[0]) / st->in_nrm0;
+    st->in_res = res;
+    if (!(res > st->in_tol) || st->total_inner >= st->max_iter)
+      st->in_stop = 1;
+    if (st->use_cond)
+      cudaGraphSetConditional((cudaGraphConditionalHandle)st->cond,
+                              st->in_stop ? 0u : 1u);
+  }
+}
+
+// d += a p; unless stopping, p = z + b p.
+__global__ void __launch_bounds__(kThreads)
+    k_inner_direction_z(int N, float *__restrict__ d, float *__restrict__ p,
+                        const float *__restrict__ z, CgState *st) {
+  if (st->in_finished) return;
+  const float a = (float)st->in_alpha, b = (float)st->in_beta;
+  const bool upd = !st->in_stop;
+  for (int i = blockIdx.x * kThreads + threadIdx.x; i < N;
+       i += gridDim.x * kThreads) {
+    const float pv = p[i];
+    d[i] = fmaf(a, pv, d[i]);
+    if (upd) p[i] = fmaf(b, pv, __ldg(&z[i]));
   }
 }
 

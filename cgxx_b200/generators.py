@@ -135,6 +135,40 @@ def gaussian_random_field(shape, sigma, corr_len, rng):
     return g
 
 
+def diffusion_field(n, sigma, corr_len, seed):
+    """exp(g) on an n^3 grid, g the Gaussian random field of diffusion3d."""
+    rng = np.random.default_rng(seed)
+    return np.exp(gaussian_random_field((n, n, n), sigma, corr_len, rng))
+
+
+class Diffusion7Family:
+    """Many 7-point matrices on one n^3 grid: the pattern (ptr, index) is
+    built once and `values(coeff)` returns the value array of diffusion3d for
+    a new coefficient field, in the same order."""
+
+    def __init__(self, n):
+        self.n = n
+        A = diffusion3d(n, stencil=7, coeff=np.ones((n, n, n)))
+        self.ptr, self.index, self.N = A.ptr, A.index, A.N
+        rows = A.rows().astype(np.int64)
+        self._rows, self._cols = rows, A.index.astype(np.int64)
+        self._diag = rows == self._cols
+        # Dirichlet ghost faces per row: 6 minus the number of neighbours.
+        self._ghost = 6 - (np.diff(A.ptr) - 1)
+
+    def values(self, coeff):
+        k = coeff.ravel().astype(np.float64)
+        ki, kj = k[self._rows], k[self._cols]
+        off = -2.0 * ki * kj / (ki + kj)
+        val = np.where(self._diag, 0.0, off)
+        diag = -np.bincount(self._rows, weights=val, minlength=self.N) + self._ghost * k
+        val[self._diag] = diag
+        return val
+
+    def matrix(self, coeff):
+        return Crs(self.N, self.ptr, self.index, self.values(coeff))
+
+
 def diffusion3d(n, stencil=7, sigma=1.0, corr_len=8.0, seed=0, coeff=None):
     """Variable-coefficient diffusion on an n^3 grid (see module docstring)."""
     shape = (n, n, n)

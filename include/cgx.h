@@ -178,6 +178,44 @@ cgx_status cgx_apply_jacobi(cgx_handle *h, cgx_vector x,
 cgx_status cgx_solve(cgx_handle *h, const cgx_options *opts,
                      cgx_result *result);
 
+/* Learned preconditioner M^-1 = G G^T + eps D^-1 (no counterpart in the
+ * reference; it extends CG_PRECONDITIONER beyond none/jacobi). G is lower
+ * triangular on the pattern of tril(A); its values come from a small
+ * message-passing network (3 layers, width 32, BF16 tensor cores with FP32
+ * accumulation) that reads the Jacobi-scaled matrix. The arithmetic is stated
+ * in oracle/gnn_oracle.py. Used by cgx_solve with
+ * preconditioner = CGX_PRECONDITIONER_LEARNED and precision = MIXED. */
+typedef struct cgx_gnn cgx_gnn;
+int cgx_gnn_param_count(void);
+/* params: cgx_gnn_param_count() floats in the oracle's layout, or NULL (0). */
+cgx_status cgx_gnn_create(cgx_gnn **out, int device, const float *params);
+cgx_status cgx_gnn_destroy(cgx_gnn *g);
+cgx_status cgx_gnn_set_params(cgx_gnn *g, const float *params);
+cgx_status cgx_gnn_get_params(cgx_gnn *g, float *params);
+/* Replaces the values of the uploaded CRS matrix (same pattern); `value`
+ * may be host or device memory. */
+cgx_status cgx_update_crs_values(cgx_handle *h, const double *value);
+/* Builds the Jacobi-scaled graph of the uploaded CRS matrix (needs positive
+ * diagonal entries and a structurally symmetric pattern). After
+ * cgx_update_crs_values it only recomputes the scaled values. */
+cgx_status cgx_learned_setup(cgx_handle *h);
+/* Network inference: G and G^T for the current matrix, eps >= 0. */
+cgx_status cgx_learned_factor(cgx_handle *h, cgx_gnn *g, double eps);
+/* Unscaled factor Ghat = D^1/2 G on its pattern (arrays of *nnzL entries,
+ * each optional). */
+cgx_status cgx_learned_get_factor(cgx_handle *h, int *nnzL, float *ghat,
+                                  int *rows, int *cols);
+/* Hutchinson loss ||(Ghat^T Ahat Ghat - I) V||_F^2 / (N S) for S = 8 probe
+ * columns (probes: N*8 floats, node-major, or NULL for Rademacher probes
+ * from `seed`) and its gradient w.r.t. the parameters (grad may be NULL). */
+cgx_status cgx_gnn_loss_grad(cgx_gnn *g, cgx_handle *h, const float *probes,
+                             unsigned long long seed, float *loss,
+                             float *grad);
+/* One Adam step on Rademacher probes from `seed`; *loss (optional) is the
+ * loss before the step. */
+cgx_status cgx_gnn_train_step(cgx_gnn *g, cgx_handle *h,
+                              unsigned long long seed, float lr, float *loss);
+
 /* FP64 ||k - A x|| / ||k|| of the current X. */
 cgx_status cgx_true_residual(cgx_handle *h, double *rel);
 

@@ -1,0 +1,194 @@
+"""The learned preconditioner on the GPU against its CPU oracle
+(oracle/gnn_oracle.py; the reference has no counterpart, so parity is pinned
+to that restatement).
+
+Tolerances: the network runs with BF16 activations on the tensor cores; the
+oracle rounds at the same points but accumulates in a different order, so a
+value that lands near a BF16 rounding boundary can round the other way.
+Factor values: max |G - G_oracle| <= 2e-2 max |G_oracle|. Gradient:
+||g - g_oracle|| <= 3e-2 ||g_oracle||, loss within 1e-3 relative.
+"""
+import numpy as np
+import pytest
+
+import cgxx_b200 as cg
+from cgxx_b200 import generators as G
+from conftest import random_crs
+from oracle import gnn_oracle as GO
+
+pytestmark = pytest.mark.gpu
+
+
+def _setup(A):
+    h = cg.Handle(0)
+    h.upload_crs(A.ptr, A.index, A.value)
+    h.upload_jacobi(1.0 / A.diagonal())
+    h.learned_setup()
+    return h
+
+
+def _oracle_factor_in_g_order(A, params, rows, cols):
+    g = GO.Graph(A.ptr, A.index, A.value)
+    gd, go = GO.factor(g, params)
+    out = np.empty(len(rows), np.float32)
+    k = 0
+    for e, (r, c) in enumerate(zip(rows, cols)):
+        if r == c:
+            out[e] = gd[r]
+        else:
+            out[e] = go[k]
+            k += 1
+    assert k == len(go)
+    return out
+
+
+def _params(seed, scale=1.0):
+    p = GO.init_params(seed)
+    rng = np.random.default_rng(seed + 100)
+    # Move away from the near-zero head so every term contributes.
+    return (p + scale * 0.05 * rng.standard_normal(p.size)).astype(np.float32)
+
+
+MATRICES = [
+    ("diffusion7_10", lambda: G.diffusion3d(10, 7, sigma=1.5, corr_len=4.0, seed=1)),
+    ("diffusion27_6", lambda: G.diffusion3d(6, 27, sigma=1.0, corr_len=3.0, seed=2)),
+    ("random_spd_500", lambda: random_crs(500, 0, 30, seed=7, spd=True)),
+]
+
+
+@pytest.mark.parametrize("name,make", MATRICES, ids=[m[0] for m in MATRICES])
+def test_factor_matches_oracle(name, make):
+    A = make()
+    h = _setup(A)
+    params = _params(3)
+    net = cg.Gnn(0, params)
+    h.learned_factor(net, 0.0)
+    ghat, rows, cols = h.learned_get_factor()
+    ref = _oracle_factor_in_g_order(A, params, rows, cols)
+    assert np.all(rows >= cols)
+    assert np.max(np.abs(ghat - ref)) <= 2e-2 * np.max(np.abs(ref))
+    assert np.median(np.abs(ghat - ref)) <= 1e-3 * np.max(np.abs(ref))
+    h.close()
+    net.close()
+
+
+@pytest.mark.parametrize("name,make", MATRICES, ids=[m[0] for m in MATRICES])
+def test_gradient_matches_oracle(name, make):
+    A = make()
+    h = _setup(A)
+    params = _params(5)
+    net = cg.Gnn(0, params)
+    V = np.random.default_rng(9).choice([-1.0, 1.0], size=(A.N, 8)).astype(np.float32)
+    loss, grad = net.loss_grad(h, probes=V)
+    lo, go = GO.loss_and_grad(GO.Graph(A.ptr, A.index, A.value), params, V)
+    assert abs(loss - lo) <= 1e-3 * abs(lo)
+    assert np.linalg.norm(grad - go) <= 3e-2 * np.linalg.norm(go)
+    # Each parameter block separately, so one block cannot hide in another.
+    o = 0
+    for pname, shp in GO.param_shapes():
+        n = int(np.prod(shp))
+        gb, rb = grad[o:o + n], go[o:o + n]
+        if np.linalg.norm(rb) > 1e-6 * np.linalg.norm(go):
+            assert np.linalg.norm(gb - rb) <= 5e-2 * np.linalg.norm(rb), pname
+        o += n
+    h.close()
+    net.close()
+
+
+def test_gradient_is_deterministic():
+    A = G.diffusion3d(12, 7, seed=4)
+    h = _setup(A)
+    net = cg.Gnn(0, _params(1))
+    l1, g1 = net.loss_grad(h, seed=77)
+    l2, g2 = net.loss_grad(h, seed=77)
+    assert l1 == l2 and np.array_equal(g1, g2)
+    h.close()
+    net.close()
+
+
+def test_training_lowers_the_loss():
+    fam = G.Diffusion7Family(12)
+    rng = np.random.default_rng(0)
+    mats = [fam.values(G.diffusion_field(12, rng.uniform(0.5, 2), rng.uniform(4, 16), 50 + k))
+            for k in range(4)]
+    h = cg.Handle(0)
+    h.upload_crs(fam.ptr, fam.index, mats[0])
+    h.learned_setup()
+    net = cg.Gnn(0, GO.init_params(0))
+
+    def mean_loss():
+        tot = 0.0
+        for v in mats:
+            h.update_crs_values(v)
+            h.learned_setup()
+            tot += net.loss_grad(h, seed=12345)[0]
+        return tot / len(mats)
+
+    before = mean_loss()
+    for step in range(60):
+        h.update_crs_values(mats[step % len(mats)])
+        h.learned_setup()
+        net.train_step(h, seed=1000 + step, lr=3e-3)
+    after = mean_loss()
+    assert after < before
+    h.close()
+    net.close()
+
+
+def _solve(h, precond, b):
+    h.set_vector("K", b)
+    h.fill_vector("X", 0.0)
+    return h.solve(max_iterations=20000, tolerance=1e-9, precision=cg.PRECISION_MIXED,
+                   preconditioner=precond)
+
+
+@pytest.mark.parametrize("loop", [cg.LOOP_GRAPH, cg.LOOP_KERNELS])
+def test_learned_solve_converges_with_fewer_iterations(loop):
+    A = G.diffusion3d(24, 7, sigma=1.0, corr_len=8.0, seed=11)
+    b, xs = G.rhs_for(A, seed=3)
+    h = _setup(A)
+    net = cg.Gnn(0, GO.init_params(0))
+    h.learned_factor(net, 1e-4)
+    h.set_vector("K", b)
+    rj = h.solve(max_iterations=20000, tolerance=1e-9, precision=cg.PRECISION_MIXED,
+                 preconditioner=cg.PRECOND_JACOBI, loop=loop)
+    h.fill_vector("X", 0.0)
+    rl = h.solve(max_iterations=20000, tolerance=1e-9, precision=cg.PRECISION_MIXED,
+                 preconditioner=cg.PRECOND_LEARNED, loop=loop)
+    x = h.get_vector("X")
+    assert rl["converged"] == 1 and rl["fell_back"] == 0
+    assert np.linalg.norm(b - A.matvec(x)) / np.linalg.norm(b) <= 1e-9
+    assert rl["iterations"] < 0.75 * rj["iterations"], (rl["iterations"], rj["iterations"])
+    h.close()
+    net.close()
+
+
+def test_corrupted_network_falls_back_to_jacobi():
+    A = G.diffusion3d(16, 7, seed=6)
+    b, _ = G.rhs_for(A, seed=2)
+    h = _setup(A)
+    p = GO.init_params(0)
+    p[GO.param_count() - 1] = np.nan  # poisons the head bias -> NaN factor
+    net = cg.Gnn(0, p)
+    h.learned_factor(net, 0.0)
+    h.set_vector("K", b)
+    r = h.solve(max_iterations=20000, tolerance=1e-9, precision=cg.PRECISION_MIXED,
+                preconditioner=cg.PRECOND_LEARNED)
+    x = h.get_vector("X")
+    assert r["fell_back"] == 1 and r["converged"] == 1
+    assert np.linalg.norm(b - A.matvec(x)) / np.linalg.norm(b) <= 1e-9
+    h.close()
+    net.close()
+
+
+def test_learned_setup_rejects_unsymmetric_pattern():
+    N = 50
+    rows = np.concatenate([np.arange(N), np.arange(1, N)])
+    cols = np.concatenate([np.arange(N), np.arange(0, N - 1)])  # lower only
+    A = G.crs_from_unsorted(N, rows, cols, np.concatenate([np.full(N, 2.0), -np.ones(N - 1)]))
+    h = cg.Handle(0)
+    h.upload_crs(A.ptr, A.index, A.value)
+    with pytest.raises(cg.CgxError) as e:
+        h.learned_setup()
+    assert "symmetric" in e.value.message
+    h.close()
