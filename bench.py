@@ -11,10 +11,16 @@ One step = one complete solve from x0 = 0 to the tolerance, inputs resident
 in device memory. The matrix (342 MB) is larger than the 126 MB L2, so no
 flush is needed between steps.
 
-Paths (--path): plain = FP64 Jacobi-PCG (the reference's arithmetic),
-mixed = FP32 inner Jacobi-PCG inside FP64 iterative refinement (stops on the
-FP64 true residual). `value` is the solve time of the path named in
-config.path; the other path's time is reported next to it.
+Paths (--path):
+  learned (default) = FP32 inner PCG with the learned factor M^-1 = G G^T +
+      eps D^-1 inside FP64 iterative refinement, stopping on the FP64 true
+      residual; every step includes the scaled-graph set-up and the network
+      inference that produce G (the weights come from --weights, else the
+      untrained initialisation, and the line says which);
+  mixed = the same refinement with FP32 Jacobi-PCG inside;
+  plain = FP64 Jacobi-PCG, the reference's arithmetic.
+`value` is the time of the path named in config.path; the other two paths'
+times are reported next to it under `paths`.
 
 --impl reference runs the reference's own OpenMP CG (oracle/_ref, built from
 the unmodified reference sources) on the box's host cores instead.
@@ -46,7 +52,10 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--n", type=int, default=160, help="grid edge (default 160)")
-    ap.add_argument("--path", choices=["plain", "mixed"], default="plain")
+    ap.add_argument("--path", choices=["learned", "mixed", "plain"], default="learned")
+    ap.add_argument("--weights", default=os.path.join(REPO, "cgxx_b200", "weights",
+                                                       "diffusion7.gnn"))
+    ap.add_argument("--eps", type=float, default=1e-4)
     ap.add_argument("--max-iter", type=int, default=5000)
     ap.add_argument("--tol", type=float, default=1e-9)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -273,14 +282,29 @@ def peaks():
 
 
 LOOPS = {"graph": 0, "chunked": 1, "kernels": 2}
+PATHS = ("learned", "mixed", "plain")
 
 
 def solve_opts(cg, args, path, loop=None):
+    pc = {"learned": cg.PRECOND_LEARNED}.get(path, cg.PRECOND_JACOBI)
+    prec = cg.PRECISION_FP64 if path == "plain" else cg.PRECISION_MIXED
     return cg.default_options(
-        max_iterations=args.max_iter, tolerance=args.tol,
-        preconditioner=cg.PRECOND_JACOBI,
-        precision=cg.PRECISION_MIXED if path == "mixed" else cg.PRECISION_FP64,
-        loop=LOOPS[args.loop] if loop is None else loop, inner_tolerance=1e-5, max_outer=30)
+        max_iterations=args.max_iter, tolerance=args.tol, preconditioner=pc,
+        precision=prec, loop=LOOPS[args.loop] if loop is None else loop,
+        inner_tolerance=1e-5, max_outer=30)
+
+
+def load_network(args):
+    """Parameters of the learned preconditioner: the trained weight file if
+    present, else the untrained initialisation (reported as such)."""
+    from cgxx_b200 import learned as LRN
+    path = args.weights
+    if path and os.path.exists(path):
+        params, head = LRN.load_weights(path)
+        return params, {"weights": os.path.relpath(path, REPO),
+                        "trained_steps": head.get("steps"),
+                        "config_sha256": head.get("config_sha256")}
+    return LRN.init_params(0), {"weights": "untrained initialisation (no weight file)"}
 
 
 def our_arm(args, world, rank, local):
@@ -290,6 +314,7 @@ def our_arm(args, world, rank, local):
 
     A, b, xs = workload(args.n)
     Cd = 1.0 / A.diagonal()
+    N, nnz = A.N, A.nz
     dev = local if world > 1 else 0
     torch.cuda.set_device(dev)
     stream = torch.cuda.Stream()
@@ -298,17 +323,25 @@ def our_arm(args, world, rank, local):
     h.upload_crs(A.ptr, A.index, A.value)
     h.upload_jacobi(Cd)
     h.set_vector("K", b)
+    params, net_info = load_network(args)
+    net = cg.Gnn(dev, params)
 
-    def one_solve(path):
+    def one_solve(path, loop=None):
+        """One complete solve from x0 = 0. The learned path includes, every
+        step, the scaled-graph set-up and the network inference of G."""
         h.fill_vector("X", 0.0)
-        return h.solve(solve_opts(cg, args, path))
+        if path == "learned":
+            h.learned_setup()
+            h.learned_factor(net, args.eps)
+        return h.solve(solve_opts(cg, args, path, loop))
 
-    # Warm-up (also builds the CUDA graphs of both paths).
+    # Warm-up (also builds the CUDA graphs of every path).
     for _ in range(args.warmup):
         one_solve(args.path)
-    other = "mixed" if args.path == "plain" else "plain"
+    others = [p for p in PATHS if p != args.path]
     if not args.quick:
-        one_solve(other)
+        for p in others:
+            one_solve(p)
 
     # Timed region: K complete solves, device-timed with CUDA events on the
     # stream the library launches on, bracketed by barrier + synchronize.
@@ -334,37 +367,79 @@ def our_arm(args, world, rank, local):
     if args.quick:
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": ms, "unit": "ms", "quick": True,
-                              "iterations": res["iterations"], "true_residual": true_rel,
-                              "config": workload_config(args, A), "clocks": clocks}))
+                              "path": args.path, "iterations": res["iterations"],
+                              "true_residual": true_rel, "config": workload_config(args, A),
+                              "clocks": clocks}))
         h.close()
         return
 
-    # The other path, for the side-by-side number.
-    oth = []
-    for _ in range(2):
-        oth.append(one_solve(other))
-    other_ms = statistics.median(r["solve_ms"] for r in oth)
+    # The other paths, side by side (median of two solves each; the learned
+    # path's time includes its set-up and inference).
+    def timed(path):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        r = one_solve(path)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1), r
 
-    # Per-launch kernel times (roofline): one solve of the plain path with
-    # every fused kernel bracketed by CUDA events.
-    h.fill_vector("X", 0.0)
-    kr = h.solve(solve_opts(cg, args, "plain", loop=cg.LOOP_KERNELS))
-    spmv_us = 1e3 * kr["spmv_ms"] / max(1, kr["spmv_launches"])
-    upd_us = 1e3 * kr["update_ms"] / max(1, kr["update_launches"])
-    dir_us = 1e3 * kr["direction_ms"] / max(1, kr["direction_launches"])
-    N, nnz = A.N, A.nz
-    spmv_bytes = 12 * nnz + 4 * (N + 1) + 16 * N   # values+cols, ptr, p once, q
-    upd_bytes = 32 * N                              # r, q, C read; r written
-    dir_bytes = 48 * N                              # x, p, r, C read; x, p written
-    iter_bytes = spmv_bytes + upd_bytes + dir_bytes
+    side = {args.path: {"ms": ms, "iterations": res["iterations"],
+                        "outer_iterations": res["outer_iterations"],
+                        "fell_back": bool(res["fell_back"])}}
+    for p in others:
+        runs = [timed(p) for _ in range(2)]
+        side[p] = {"ms": statistics.median(t for t, _ in runs),
+                   "iterations": runs[-1][1]["iterations"],
+                   "outer_iterations": runs[-1][1]["outer_iterations"],
+                   "fell_back": bool(runs[-1][1]["fell_back"])}
+    # Learned path: network set-up + inference alone.
+    fe0 = torch.cuda.Event(enable_timing=True)
+    fe1 = torch.cuda.Event(enable_timing=True)
+    fe0.record(stream)
+    h.learned_setup()
+    h.learned_factor(net, args.eps)
+    fe1.record(stream)
+    torch.cuda.synchronize()
+    side["learned"]["factor_ms"] = fe0.elapsed_time(fe1)
+
+    # Per-launch kernel times (roofline), one solve per path with every fused
+    # kernel bracketed by CUDA events.
+    kern = {}
+    for p in ("plain", args.path) if args.path != "plain" else ("plain",):
+        r = one_solve(p, loop=cg.LOOP_KERNELS)
+        kern[p] = {"spmv_us": 1e3 * r["spmv_ms"] / max(1, r["spmv_launches"]),
+                   "update_us": 1e3 * r["update_ms"] / max(1, r["update_launches"]),
+                   "direction_us": 1e3 * r["direction_ms"] / max(1, r["direction_launches"]),
+                   "launches": r["spmv_launches"]}
     peak, peak_kind = peaks()
-    achieved = spmv_bytes / (spmv_us * 1e-6) / 1e9
-    iter_us = spmv_us + upd_us + dir_us
+    fp64_spmv_bytes = 12 * nnz + 4 * (N + 1) + 16 * N  # values+cols, ptr, p once, q
+    fp32_spmv_bytes = 8 * nnz + 4 * (N + 1) + 8 * N
+    plain_iter_bytes = fp64_spmv_bytes + 32 * N + 48 * N
+    kp = kern["plain"]
+    plain_iter_us = kp["spmv_us"] + kp["update_us"] + kp["direction_us"]
+    fp64_roof = {"bound": "hbm", "achieved": fp64_spmv_bytes / (kp["spmv_us"] * 1e-6) / 1e9,
+                 "peak": peak, "unit": "GB/s",
+                 "kernel": "k_crs<double, OpPcgQ>: q = A p fused with <p,q> (FP64 CRS)",
+                 "algorithmic_bytes": fp64_spmv_bytes, "peak_kind": peak_kind}
+    fp64_roof["frac"] = fp64_roof["achieved"] / peak
     prof = read_traffic_profile("spmv_crs_fp64_diffusion7_160.json")
-    traffic = prof.get("dram_bytes_per_launch") if prof else None
+    fp64_roof["traffic"] = prof.get("dram_bytes_per_launch") if prof else None
+    if args.path == "plain":
+        roof = fp64_roof
+    else:
+        kk = kern[args.path]
+        roof = {"bound": "hbm", "achieved": fp32_spmv_bytes / (kk["spmv_us"] * 1e-6) / 1e9,
+                "peak": peak, "unit": "GB/s",
+                "kernel": "k_crs<float, OpInnerQ>: q = A p fused with <p,q> (FP32 CRS, inner)",
+                "algorithmic_bytes": fp32_spmv_bytes, "peak_kind": peak_kind}
+        roof["frac"] = roof["achieved"] / peak
+        prof32 = read_traffic_profile("spmv_crs_fp32_diffusion7_160.json")
+        roof["traffic"] = prof32.get("dram_bytes_per_launch") if prof32 else None
 
     # End to end through the public C ABI: pinned host inputs uploaded every
-    # step (matrix, Jacobi C, right-hand side), solve, read back x.
+    # step (matrix, Jacobi C, right-hand side), the learned set-up and
+    # inference, the solve, x read back.
     ptr_h = cg.pinned_empty(N + 1, np.int32)
     idx_h = cg.pinned_empty(nnz, np.int32)
     val_h = cg.pinned_empty(nnz, np.float64)
@@ -382,21 +457,19 @@ def our_arm(args, world, rank, local):
         h.upload_crs(ptr_h, idx_h, val_h)
         h.upload_jacobi(c_h)
         h.set_vector("K", b_h)
+        if args.path == "learned":
+            h.learned_setup()
+            h.learned_factor(net, args.eps)
         r = h.solve(solve_opts(cg, args, args.path))
-        out = h.get_vector("X")
-        x_h[:] = out
+        x_h[:] = h.get_vector("X")
         return r
 
-    e2e_step()  # warm-up (graph build after re-upload)
+    e2e_step()  # warm-up (graphs are rebuilt after a re-upload)
     barrier(world)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
     for _ in range(e2e_steps):
         e2e_step()
-    e1.record(stream)
     torch.cuda.synchronize()
     wall_ms = (time.perf_counter() - t0) * 1e3 / e2e_steps
     barrier(world)
@@ -405,36 +478,36 @@ def our_arm(args, world, rank, local):
     d2h = 8 * N
 
     iters = res["iterations"]
+    outer = res["outer_iterations"]
     if args.path == "plain":
-        launches = args.steps * (1 + 1 + 4 * iters)  # fill, setup, 3 fused + guard
+        per_solve = 2 + 4 * iters                   # fill, set-up, 3 fused + guard
+    elif args.path == "mixed":
+        per_solve = 2 + 3 * outer + 1 + 4 * iters   # dot, true residuals, start, update
     else:
-        outer = res["outer_iterations"]
-        launches = args.steps * (1 + 1 + (outer + 1) + outer * 2 + 4 * iters)
+        per_solve = 2 + 19 + 3 * outer + 1 + 3 * outer + 7 * iters  # + set-up, network
+    launches = args.steps * per_solve
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(A, b, args, iters if args.path == "plain" else None)
+        cpu = cpu_baseline(A, b, args, side["plain"]["iterations"])
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": ms, "unit": "ms", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64" if args.path == "plain" else "f32+f64",
+            "dtype": {"plain": "f64", "mixed": "f32+f64"}.get(args.path, "bf16+f32+f64"),
             "data": "synthetic (seeded generator; no dataset)",
-            "config": workload_config(args, A),
-            "iterations": iters, "outer_iterations": res["outer_iterations"],
+            "config": dict(workload_config(args, A), network=net_info),
+            "iterations": iters, "outer_iterations": outer,
             "residual": res["residual"], "true_residual": true_rel,
             "rel_error_vs_exact": err_vs_exact, "converged": bool(res["converged"]),
-            "other_path": {"path": other, "ms": other_ms,
-                           "iterations": oth[-1]["iterations"]},
-            "kernel_us": {"spmv_fused_dot": spmv_us, "update": upd_us,
-                          "direction": dir_us, "iteration": iter_us},
-            "iteration_gbs": iter_bytes / (iter_us * 1e-6) / 1e9,
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak,
-                         "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
-                         "kernel": "k_crs<double, OpPcgQ> (q = A p fused with <p,q>)",
-                         "algorithmic_bytes": spmv_bytes, "peak_kind": peak_kind},
+            "paths": side,
+            "speedup_vs_plain_fp64": side["plain"]["ms"] / ms,
+            "kernel_us": kern,
+            "plain_iteration_gbs": plain_iter_bytes / (plain_iter_us * 1e-6) / 1e9,
+            "roofline": roof,
+            "roofline_fp64_spmv": fp64_roof,
             "clocks": clocks,
             "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "steps": e2e_steps},
@@ -443,6 +516,7 @@ def our_arm(args, world, rank, local):
         }
         print(json.dumps(line))
     h.close()
+    net.close()
 
 
 def cpu_baseline(A, b, args, full_iters):

@@ -140,6 +140,11 @@ struct cgx_handle {
   // FP32 mirror and inner vectors of the mixed path (allocated on demand).
   void *f32_mem = nullptr;
   float *value32 = nullptr, *C32 = nullptr;
+  // Column indices as 16-bit offsets from the row, when they all fit
+  // (compact16): the mixed and learned paths read 6 instead of 8 bytes per
+  // FP32 entry.
+  int16_t *idx16 = nullptr;
+  bool compact16 = false;
   float *d32 = nullptr, *r32 = nullptr, *p32 = nullptr, *q32 = nullptr;
   double *r64 = nullptr;
   bool f32_valid = false;
@@ -171,6 +176,9 @@ struct Learned {
   int *gptr = nullptr, *gcol = nullptr, *grow = nullptr, *g2a = nullptr;
   int *tptr = nullptr, *tcol = nullptr, *t2g = nullptr, *g2t = nullptr;
   float *ghat = nullptr, *gs = nullptr, *gts = nullptr;
+  // Compact copies for the apply: BF16 values, 16-bit column offsets.
+  __nv_bfloat16 *gsb = nullptr, *gtsb = nullptr;
+  int16_t *gcol16 = nullptr, *tcol16 = nullptr;
   __nv_bfloat16 *h[4] = {};
   __nv_bfloat16 *agg[3] = {};
   float *pre[4] = {};
@@ -231,6 +239,8 @@ static void free_matrix(cgx_handle *h) {
   h->c_valid = false;
   h->value32 = h->C32 = h->d32 = h->r32 = h->p32 = h->q32 = nullptr;
   h->r64 = nullptr;
+  h->idx16 = nullptr;
+  h->compact16 = false;
   h->f32_valid = false;
 }
 
@@ -300,12 +310,12 @@ __global__ void k_loop_guard(CgState *st) {
 
 // Staged CRS SpMV over any CRS view (A itself, or the learned factor's G and
 // G^T, whose rows are subsets of A's rows so A's tile capacity bounds them).
-template <typename VT, typename Op>
-static cudaError_t launch_crs_view(cgx_handle *h, CrsView<VT> A, const VT *x,
-                                   Op op) {
+template <typename VT, typename IT, typename Op>
+static cudaError_t launch_crs_view(cgx_handle *h, CrsView<VT, IT> A,
+                                   const typename Comp<VT>::T *x, Op op) {
   const int cap = A.tile_cap;
-  const size_t smem = crs_smem_bytes<VT>(cap);
-  auto kern = k_crs<VT, Op>;
+  const size_t smem = crs_smem_bytes<VT, IT>(cap);
+  auto kern = k_crs<VT, IT, Op>;
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(
         kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -326,8 +336,8 @@ static cudaError_t launch_crs_view(cgx_handle *h, CrsView<VT> A, const VT *x,
 template <typename VT, typename Op>
 static cudaError_t launch_crs(cgx_handle *h, const VT *value, int cap,
                               const VT *x, Op op) {
-  return launch_crs_view<VT, Op>(h, CrsView<VT>{h->ptr, h->index, value, h->N, cap},
-                                 x, op);
+  return launch_crs_view<VT, int, Op>(
+      h, CrsView<VT, int>{h->ptr, h->index, value, h->N, cap}, x, op);
 }
 
 template <typename Op>
@@ -396,14 +406,24 @@ static cudaError_t launch_pcg_setup(cgx_handle *h, bool jacobi) {
                      OpSetup<false>{k, r, p, h->C, ticket(h, kTicketSetup)});
 }
 
+// q = A p in FP32 with <p,q> (inner solves), compact indices when they fit.
+static cudaError_t launch_inner_q(cgx_handle *h) {
+  OpInnerQ op{h->p32, h->q32, ticket(h, kTicketInnerQ)};
+  if (h->compact16)
+    return launch_crs_view(
+        h, CrsView<float, int16_t>{h->ptr, h->idx16, h->value32, h->N, h->tile_cap},
+        h->p32, op);
+  return launch_crs_view(
+      h, CrsView<float, int>{h->ptr, h->index, h->value32, h->N, h->tile_cap},
+      h->p32, op);
+}
+
 // Inner FP32 PCG iteration of the mixed path.
 static cudaError_t launch_inner_iteration(cgx_handle *h,
                                           cudaEvent_t *evs = nullptr) {
   cudaError_t e;
   if (evs) cudaEventRecord(evs[0], h->stream);
-  e = launch_crs<float, OpInnerQ>(
-      h, h->value32, h->tile_cap, h->p32,
-      OpInnerQ{h->p32, h->q32, ticket(h, kTicketInnerQ)});
+  e = launch_inner_q(h);
   if (e != cudaSuccess) return e;
   if (evs) cudaEventRecord(evs[1], h->stream);
   const int g = grid_stream(h, (size_t)(h->N + 3) / 4);
@@ -1163,6 +1183,7 @@ static cgx_status ensure_f32(cgx_handle *h) {
     size_t o_p = c.take<float>((size_t)N + kPad);
     size_t o_q = c.take<float>((size_t)N + kPad);
     size_t o_r64 = c.take<double>((size_t)N + kPad);
+    size_t o_i16 = c.take<int16_t>((size_t)h->nz + kPad);
     CUDA_TRY(cudaMalloc(&h->f32_mem, c.off));
     CUDA_TRY(cudaMemsetAsync(h->f32_mem, 0, c.off, h->stream));
     char *base = (char *)h->f32_mem;
@@ -1173,6 +1194,7 @@ static cgx_status ensure_f32(cgx_handle *h) {
     h->p32 = (float *)(base + o_p);
     h->q32 = (float *)(base + o_q);
     h->r64 = (double *)(base + o_r64);
+    h->idx16 = (int16_t *)(base + o_i16);
   }
   k_to_f32<<<grid_stream(h, h->nz), kThreads, 0, h->stream>>>(
       (size_t)h->nz, h->value, h->value32);
@@ -1180,6 +1202,15 @@ static cgx_status ensure_f32(cgx_handle *h) {
   k_to_f32<<<grid_stream(h, N), kThreads, 0, h->stream>>>((size_t)N, h->C,
                                                           h->C32);
   CUDA_TRY(cudaGetLastError());
+  CUDA_TRY(cudaMemsetAsync(h->flag, 0, sizeof(int), h->stream));
+  k_delta16<<<grid_stream(h, N), kThreads, 0, h->stream>>>(N, h->ptr, h->index,
+                                                           h->idx16, h->flag);
+  CUDA_TRY(cudaGetLastError());
+  CUDA_TRY(cudaMemcpyAsync(h->host_scalar, h->flag, sizeof(int),
+                           cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  h->compact16 = *(int *)h->host_scalar == 0;
+  drop_graphs(h);  // the inner graphs depend on the index form
   h->f32_valid = true;
   return CGX_SUCCESS;
 }
@@ -1199,14 +1230,21 @@ static cgx_status true_residual_r2(cgx_handle *h, double *r2) {
 // z = G (G^T r) + eps C r with <r,z> (start: also p = z and rho).
 static cudaError_t launch_learned_apply(cgx_handle *h, bool start) {
   Learned *L = h->L;
-  CrsView<float> GT{L->tptr, L->tcol, L->gts, h->N, h->tile_cap};
-  CrsView<float> Gv{L->gptr, L->gcol, L->gs, h->N, h->tile_cap};
-  cudaError_t e = launch_crs_view<float>(h, GT, h->r32, OpInnerStore{L->y32});
+  const OpLearnedZ zop{h->r32, h->C32, L->z32, h->p32, L->eps, start ? 1 : 0,
+                       ticket(h, kTicketInnerStart)};
+  cudaError_t e;
+  if (h->compact16) {
+    CrsView<__nv_bfloat16, int16_t> GT{L->tptr, L->tcol16, L->gtsb, h->N, h->tile_cap};
+    CrsView<__nv_bfloat16, int16_t> Gv{L->gptr, L->gcol16, L->gsb, h->N, h->tile_cap};
+    e = launch_crs_view(h, GT, h->r32, OpInnerStore{L->y32});
+    if (e != cudaSuccess) return e;
+    return launch_crs_view(h, Gv, L->y32, zop);
+  }
+  CrsView<float, int> GT{L->tptr, L->tcol, L->gts, h->N, h->tile_cap};
+  CrsView<float, int> Gv{L->gptr, L->gcol, L->gs, h->N, h->tile_cap};
+  e = launch_crs_view(h, GT, h->r32, OpInnerStore{L->y32});
   if (e != cudaSuccess) return e;
-  return launch_crs_view<float>(
-      h, Gv, L->y32,
-      OpLearnedZ{h->r32, h->C32, L->z32, h->p32, L->eps, start ? 1 : 0,
-                 ticket(h, kTicketInnerStart)});
+  return launch_crs_view(h, Gv, L->y32, zop);
 }
 
 static cudaError_t launch_learned_start(cgx_handle *h) {
@@ -1222,9 +1260,7 @@ static cudaError_t launch_learned_iteration(cgx_handle *h,
                                             cudaEvent_t *evs = nullptr) {
   cudaError_t e;
   if (evs) cudaEventRecord(evs[0], h->stream);
-  e = launch_crs<float, OpInnerQ>(
-      h, h->value32, h->tile_cap, h->p32,
-      OpInnerQ{h->p32, h->q32, ticket(h, kTicketInnerQ)});
+  e = launch_inner_q(h);
   if (e != cudaSuccess) return e;
   if (evs) cudaEventRecord(evs[1], h->stream);
   const int g = grid_stream(h, h->N);
@@ -1450,10 +1486,10 @@ cgx_status learned_alloc(cgx_handle *h, int nnzL) {
   size_t o_t2g = take_n<int>(c, nnzL), o_g2t = take_n<int>(c, nnzL);
   size_t o_ghat = take_n<float>(c, nnzL), o_gs = take_n<float>(c, nnzL);
   size_t o_gts = take_n<float>(c, nnzL);
-  size_t o_h[4], o_agg[3], o_pre[4];
+  size_t o_gsb = take_n<__nv_bfloat16>(c, nnzL), o_gtsb = take_n<__nv_bfloat16>(c, nnzL);
+  size_t o_gc16 = take_n<int16_t>(c, nnzL), o_tc16 = take_n<int16_t>(c, nnzL);
+  size_t o_h[4];
   for (int k = 0; k < 4; k++) o_h[k] = take_n<__nv_bfloat16>(c, (size_t)N * W);
-  for (int k = 0; k < 3; k++) o_agg[k] = take_n<__nv_bfloat16>(c, (size_t)N * W);
-  for (int k = 0; k < 4; k++) o_pre[k] = take_n<float>(c, (size_t)N * W);
   size_t o_o = take_n<float>(c, (size_t)N * NOUT);
   size_t o_y = take_n<float>(c, N), o_z = take_n<float>(c, N);
   size_t o_xb = take_n<double>(c, N);
@@ -1478,9 +1514,11 @@ cgx_status learned_alloc(cgx_handle *h, int nnzL) {
   L->ghat = (float *)(b + o_ghat);
   L->gs = (float *)(b + o_gs);
   L->gts = (float *)(b + o_gts);
+  L->gsb = (__nv_bfloat16 *)(b + o_gsb);
+  L->gtsb = (__nv_bfloat16 *)(b + o_gtsb);
+  L->gcol16 = (int16_t *)(b + o_gc16);
+  L->tcol16 = (int16_t *)(b + o_tc16);
   for (int k = 0; k < 4; k++) L->h[k] = (__nv_bfloat16 *)(b + o_h[k]);
-  for (int k = 0; k < 3; k++) L->agg[k] = (__nv_bfloat16 *)(b + o_agg[k]);
-  for (int k = 0; k < 4; k++) L->pre[k] = (float *)(b + o_pre[k]);
   L->o = (float *)(b + o_o);
   L->y32 = (float *)(b + o_y);
   L->z32 = (float *)(b + o_z);
@@ -1503,6 +1541,9 @@ cgx_status learned_train_alloc(cgx_handle *h) {
   o[k++] = take_n<float>(c, NPARAMS);                 // grad
   o[k++] = take_n<float>(c, 4);                       // loss
   o[k++] = take_n<float>(c, 2 * (W * W + W));         // gtmp
+  size_t o_agg[3], o_pre[4];
+  for (int q = 0; q < 3; q++) o_agg[q] = take_n<__nv_bfloat16>(c, (size_t)N * W);
+  for (int q = 0; q < 4; q++) o_pre[q] = take_n<float>(c, (size_t)N * W);
   CUDA_TRY(cudaMalloc(&L->train, c.off));
   CUDA_TRY(cudaMemsetAsync(L->train, 0, c.off, h->stream));
   char *b = (char *)L->train;
@@ -1524,6 +1565,8 @@ cgx_status learned_train_alloc(cgx_handle *h) {
   L->grad = (float *)(b + o[k++]);
   L->loss = (float *)(b + o[k++]);
   L->gtmp = (float *)(b + o[k++]);
+  for (int q = 0; q < 3; q++) L->agg[q] = (__nv_bfloat16 *)(b + o_agg[q]);
+  for (int q = 0; q < 4; q++) L->pre[q] = (float *)(b + o_pre[q]);
   return CGX_SUCCESS;
 }
 
@@ -1533,19 +1576,24 @@ cudaError_t gnn_forward(cgx_handle *h, const float *P, bool scaled) {
   Learned *L = h->L;
   const int N = h->N;
   cudaStream_t s = h->stream;
-  k_embed<<<grid_for(h, (size_t)N * W), kThreads, 0, s>>>(N, L->feat, P, L->h[0],
-                                                          L->pre[0]);
+  // Inference (scaled) keeps no pre-activations or aggregates: only the
+  // backward pass needs them.
+  const bool keep = !scaled;
+  k_embed<<<grid_for(h, (size_t)N * W), kThreads, 0, s>>>(
+      N, L->feat, P, L->h[0], keep ? L->pre[0] : nullptr);
   const int groups = (N + 15) / 16;
   const int lgrid = std::max(
       1, std::min(h->num_sms * 8, (groups + kLayerWarps - 1) / kLayerWarps));
   for (int l = 0; l < 3; l++)
     k_layer<<<lgrid, 32 * kLayerWarps, 0, s>>>(N, h->ptr, h->index, L->ahat, P,
                                                l, L->h[l], L->h[l + 1],
-                                               L->agg[l], L->pre[l + 1]);
+                                               keep ? L->agg[l] : nullptr,
+                                               keep ? L->pre[l + 1] : nullptr);
   k_head<<<grid_for(h, (size_t)N * NOUT), kThreads, 0, s>>>(N, L->h[3], P, L->o);
   k_assemble<<<grid_for(h, L->nnzL), kThreads, 0, s>>>(
       L->nnzL, L->grow, L->gcol, L->g2a, L->ahat, L->o, L->ghat, L->dis,
-      L->g2t, scaled ? L->gs : nullptr, scaled ? L->gts : nullptr);
+      L->g2t, scaled ? L->gs : nullptr, scaled ? L->gts : nullptr,
+      scaled ? L->gsb : nullptr, scaled ? L->gtsb : nullptr);
   return cudaGetLastError();
 }
 
@@ -1794,6 +1842,14 @@ cgx_status cgx_learned_setup(cgx_handle *h) {
   k_transpose_map<<<grid_stream(h, L->nnzL), kThreads, 0, s>>>(
       L->nnzL, L->grow, L->gcol, L->tptr, L->tcol, L->g2t, L->t2g, L->flag);
   CUDA_TRY(cudaGetLastError());
+  {
+    // 16-bit column offsets of G and G^T (used when A's fit, see ensure_f32).
+    int *f16 = L->flag + 1;
+    CUDA_TRY(cudaMemsetAsync(f16, 0, sizeof(int), s));
+    k_delta16<<<g, kThreads, 0, s>>>(N, L->gptr, L->gcol, L->gcol16, f16);
+    k_delta16<<<g, kThreads, 0, s>>>(N, L->tptr, L->tcol, L->tcol16, f16);
+    CUDA_TRY(cudaGetLastError());
+  }
   CUDA_TRY(cudaMemcpyAsync(h->host_scalar, L->flag, sizeof(int),
                            cudaMemcpyDeviceToHost, s));
   CUDA_TRY(cudaStreamSynchronize(s));

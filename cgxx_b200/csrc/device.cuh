@@ -3,6 +3,8 @@
 // shared memory, and the solver state that lives in device memory.
 #pragma once
 
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 

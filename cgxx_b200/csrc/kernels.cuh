@@ -22,14 +22,36 @@ namespace cgx {
 // Matrix views (device pointers). Index/value arrays carry kPad elements of
 // padding so that 16-byte-rounded bulk copies stay inside the allocation.
 
-template <typename VT>
+// CRS with value storage VT (double, float or half) and index storage IT:
+// int holds the column itself, int16_t the column minus the row (used when
+// every entry lies within 32767 of the diagonal, which halves index bytes).
+template <typename VT, typename IT = int>
 struct CrsView {
   const int *ptr;
-  const int *index;
+  const IT *index;
   const VT *value;
   int N;
   int tile_cap;  // max nonzeros of a staged 256-row tile; 0 disables staging
 };
+
+// Arithmetic type of a value storage type: half values are widened to FP32.
+template <typename VT>
+struct Comp {
+  using T = VT;
+};
+template <>
+struct Comp<__half> {
+  using T = float;
+};
+template <>
+struct Comp<__nv_bfloat16> {
+  using T = float;
+};
+
+__device__ __forceinline__ int column(int, int stored) { return stored; }
+__device__ __forceinline__ int column(int row, int16_t stored) {
+  return row + (int)stored;
+}
 
 template <typename VT>
 struct EllView {
@@ -47,6 +69,12 @@ __device__ __forceinline__ double madd(double acc, double v, double x) {
 }
 __device__ __forceinline__ float madd(float acc, float v, float x) {
   return fmaf(v, x, acc);
+}
+__device__ __forceinline__ float madd(float acc, __half v, float x) {
+  return fmaf(__half2float(v), x, acc);
+}
+__device__ __forceinline__ float madd(float acc, __nv_bfloat16 v, float x) {
+  return fmaf(__bfloat162float(v), x, acc);
 }
 
 template <typename VT>
@@ -85,17 +113,17 @@ __device__ __forceinline__ VT row_sum(int j0, int j1, ValF val, ColF col,
 // Row sum from shared-memory staged values/indices: the U gathers of x of a
 // group are issued first (only they occupy registers); the values are read
 // from shared memory just before each multiply-add, in entry order.
-template <typename VT, int U>
-__device__ __forceinline__ VT row_sum_staged(int j0, int j1,
+template <typename VT, typename IT, int U, typename XT = typename Comp<VT>::T>
+__device__ __forceinline__ XT row_sum_staged(int row, int j0, int j1,
                                              const VT *__restrict__ sv,
-                                             const int *__restrict__ si,
-                                             const VT *__restrict__ x) {
-  VT sum = 0;
+                                             const IT *__restrict__ si,
+                                             const XT *__restrict__ x) {
+  XT sum = 0;
   for (int j = j0; j < j1; j += U) {
-    VT xv[U];
+    XT xv[U];
 #pragma unroll
     for (int k = 0; k < U; k++)
-      if (j + k < j1) xv[k] = __ldg(&x[si[j + k]]);
+      if (j + k < j1) xv[k] = __ldg(&x[column(row, si[j + k])]);
 #pragma unroll
     for (int k = 0; k < U; k++)
       if (j + k < j1) sum = madd(sum, sv[j + k], xv[k]);
@@ -113,14 +141,17 @@ __device__ __forceinline__ VT row_sum_serial(int j0, int j1, ValF val,
   return sum;
 }
 
-// Dynamic shared memory of the staged CRS kernel for a given tile capacity.
-template <typename VT>
+// Dynamic shared memory of the staged CRS kernel for a given tile capacity:
+// two stages of cap + 16 values and indices (room for the 16-byte rounding
+// of both ends of a tile's range).
+template <typename VT, typename IT = int>
 __host__ __device__ inline size_t crs_stage_bytes(int cap) {
-  return align16((size_t)(cap + 8) * sizeof(VT)) + align16((size_t)(cap + 8) * 4);
+  return align16((size_t)(cap + 16) * sizeof(VT)) +
+         align16((size_t)(cap + 16) * sizeof(IT));
 }
-template <typename VT>
+template <typename VT, typename IT = int>
 __host__ __device__ inline size_t crs_smem_bytes(int cap) {
-  return cap > 0 ? 16 + 2 * crs_stage_bytes<VT>(cap) : 16;
+  return cap > 0 ? 16 + 2 * crs_stage_bytes<VT, IT>(cap) : 16;
 }
 
 // ---------------------------------------------------------------------------
@@ -131,23 +162,25 @@ __host__ __device__ inline size_t crs_smem_bytes(int cap) {
 // mbarriers; the x gathers go through the read-only path and mostly hit L2.
 // Tiles whose range exceeds tile_cap are read straight from global memory.
 
-template <typename VT, typename Op>
+template <typename VT, typename IT, typename Op,
+          typename XT = typename Comp<VT>::T>
 __global__ void __launch_bounds__(kThreads)
-    k_crs(CrsView<VT> A, const VT *__restrict__ x, Op op, CgState *st,
+    k_crs(CrsView<VT, IT> A, const XT *__restrict__ x, Op op, CgState *st,
           double *partials) {
   if (op.skip(st)) return;
   extern __shared__ __align__(16) unsigned char smem[];
   constexpr int VPER = vals_per_16B<VT>();
+  constexpr int IPER = vals_per_16B<IT>();
   const int cap = A.tile_cap;
   const int N = A.N;
   const int nTiles = (N + kThreads - 1) / kThreads;
   uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
-  const size_t vbytes = align16((size_t)(cap + 8) * sizeof(VT));
-  const size_t sbytes = crs_stage_bytes<VT>(cap);
+  const size_t vbytes = align16((size_t)(cap + 16) * sizeof(VT));
+  const size_t sbytes = crs_stage_bytes<VT, IT>(cap);
   VT *sval0 = reinterpret_cast<VT *>(smem + 16);
-  int *sidx0 = reinterpret_cast<int *>(smem + 16 + vbytes);
+  IT *sidx0 = reinterpret_cast<IT *>(smem + 16 + vbytes);
   VT *sval1 = reinterpret_cast<VT *>(smem + 16 + sbytes);
-  int *sidx1 = reinterpret_cast<int *>(smem + 16 + sbytes + vbytes);
+  IT *sidx1 = reinterpret_cast<IT *>(smem + 16 + sbytes + vbytes);
 
   if (cap > 0 && threadIdx.x == 0) {
     mbar_init(&bars[0], 1);
@@ -162,9 +195,9 @@ __global__ void __launch_bounds__(kThreads)
     const int s = __ldg(&A.ptr[r0]), e = __ldg(&A.ptr[r1]);
     if (!(cap > 0 && e > s && e - s <= cap)) return;
     const int vs = s & ~(VPER - 1), ve = (e + VPER - 1) & ~(VPER - 1);
-    const int is = s & ~3, ie = (e + 3) & ~3;
+    const int is = s & ~(IPER - 1), ie = (e + IPER - 1) & ~(IPER - 1);
     const unsigned vb = (unsigned)(ve - vs) * (unsigned)sizeof(VT);
-    const unsigned ib = (unsigned)(ie - is) * 4u;
+    const unsigned ib = (unsigned)(ie - is) * (unsigned)sizeof(IT);
     mbar_arrive_expect_tx(&bars[buf], vb + ib);
     bulk_g2s(buf ? sval1 : sval0, A.value + vs, vb, &bars[buf]);
     bulk_g2s(buf ? sidx1 : sidx0, A.index + is, ib, &bars[buf]);
@@ -192,23 +225,40 @@ __global__ void __launch_bounds__(kThreads)
     const int row = r0 + threadIdx.x;
     if (row < r1) {
       const int j0 = __ldg(&A.ptr[row]), j1 = __ldg(&A.ptr[row + 1]);
-      VT sum = 0;
+      XT sum = 0;
       if (staged) {
         if (ok) {
           const VT *sv = (buf ? sval1 : sval0) - (s & ~(VPER - 1));
-          const int *si = (buf ? sidx1 : sidx0) - (s & ~3);
-          sum = row_sum_staged<VT, 8>(j0, j1, sv, si, x);
+          const IT *si = (buf ? sidx1 : sidx0) - (s & ~(IPER - 1));
+          sum = row_sum_staged<VT, IT, 8>(row, j0, j1, sv, si, x);
         }
       } else {
-        sum = row_sum_serial<VT>(
-            j0, j1, [&](int j) { return __ldg(&A.value[j]); },
-            [&](int j) { return __ldg(&A.index[j]); }, x);
+        for (int j = j0; j < j1; j++)
+          sum = madd(sum, A.value[j], __ldg(&x[column(row, A.index[j])]));
       }
       op.row(row, sum, acc);
     }
     __syncthreads();
   }
   op.finish(acc, st, partials);
+}
+
+// Column indices as 16-bit offsets from the row (the compact CRS of the
+// mixed and learned paths); sets *flag if an offset does not fit.
+__global__ void __launch_bounds__(kThreads)
+    k_delta16(int N, const int *__restrict__ ptr, const int *__restrict__ index,
+              int16_t *__restrict__ out, int *flag) {
+  for (int i = blockIdx.x * kThreads + threadIdx.x; i < N;
+       i += gridDim.x * kThreads)
+    for (int j = ptr[i]; j < ptr[i + 1]; j++) {
+      const int d = index[j] - i;
+      if (d < -32768 || d > 32767) {
+        atomicOr(flag, 1);
+        out[j] = 0;
+      } else {
+        out[j] = (int16_t)d;
+      }
+    }
 }
 
 // ---------------------------------------------------------------------------

@@ -355,7 +355,8 @@ __global__ void k_assemble(int nnzL, const int *__restrict__ grow,
                            const float *__restrict__ o, float *__restrict__ ghat,
                            const double *__restrict__ dis,
                            const int *__restrict__ g2t, float *__restrict__ gs,
-                           float *__restrict__ gts) {
+                           float *__restrict__ gts, __nv_bfloat16 *__restrict__ gsb,
+                           __nv_bfloat16 *__restrict__ gtsb) {
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nnzL;
        e += gridDim.x * blockDim.x) {
     const int i = grow[e], j = gcol[e];
@@ -374,6 +375,11 @@ __global__ void k_assemble(int nnzL, const int *__restrict__ grow,
       const float sv = (float)(dis[i] * (double)v);
       gs[e] = sv;
       gts[g2t[e]] = sv;
+      if (gsb) {
+        const __nv_bfloat16 bv = __float2bfloat16_rn(sv);
+        gsb[e] = bv;
+        gtsb[g2t[e]] = bv;
+      }
     }
   }
 }

@@ -150,9 +150,7 @@ def run_training(a):
     t0 = time.time()
     tr_specs = family_specs(a.train, 100000, 1000 + a.seed)
     ho_specs = family_specs(a.heldout, 900000, 2000 + a.seed)
-    tr_vals = generate_values(a.n, tr_specs, a.workers)
     ho_vals = generate_values(a.n, ho_specs, a.workers)
-    gen_s = time.time() - t0
 
     import torch
 
@@ -160,9 +158,15 @@ def run_training(a):
     from cgxx_b200 import generators as G
     fam = G.Diffusion7Family(a.n)
     dev = torch.device("cuda", 0)
-    # All training matrices resident in HBM (N nnz doubles each).
-    tr_dev = [torch.from_numpy(v).to(dev) for v in tr_vals]
-    del tr_vals
+    # All training matrices resident in HBM (nnz doubles each), generated in
+    # batches so that the host holds one batch at a time.
+    tr_dev = []
+    if not a.eval_only:
+        for b0 in range(0, len(tr_specs), 64):
+            batch = generate_values(a.n, tr_specs[b0:b0 + 64], a.workers)
+            tr_dev += [torch.from_numpy(v).to(dev) for v in batch]
+            del batch
+    gen_s = time.time() - t0
     h = cg.Handle(0)
     h.upload_crs(fam.ptr, fam.index, ho_vals[0])
     h.learned_setup()
