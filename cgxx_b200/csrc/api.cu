@@ -176,9 +176,13 @@ struct Learned {
   int *gptr = nullptr, *gcol = nullptr, *grow = nullptr, *g2a = nullptr;
   int *tptr = nullptr, *tcol = nullptr, *t2g = nullptr, *g2t = nullptr;
   float *ghat = nullptr, *gs = nullptr, *gts = nullptr;
-  // Compact copies for the apply: BF16 values, 16-bit column offsets.
-  __nv_bfloat16 *gsb = nullptr, *gtsb = nullptr;
-  int16_t *gcol16 = nullptr, *tcol16 = nullptr;
+  // SELL-32 copies of G and G^T for the apply (BF16 values, 16-bit column
+  // offsets), used when every offset fits (sell_ok).
+  void *sell_mem = nullptr;
+  bool sell_ok = false;
+  int *sg_ptr = nullptr, *st_ptr = nullptr, *g2sg = nullptr, *t2st = nullptr;
+  int16_t *sg_col = nullptr, *st_col = nullptr;
+  __nv_bfloat16 *sg_val = nullptr, *st_val = nullptr;
   __nv_bfloat16 *h[4] = {};
   __nv_bfloat16 *agg[3] = {};
   float *pre[4] = {};
@@ -214,6 +218,7 @@ static void free_learned(cgx_handle *h) {
   if (!h->L) return;
   if (h->L->mem) cudaFree(h->L->mem);
   if (h->L->train) cudaFree(h->L->train);
+  if (h->L->sell_mem) cudaFree(h->L->sell_mem);
   delete h->L;
   h->L = nullptr;
 }
@@ -1233,12 +1238,17 @@ static cudaError_t launch_learned_apply(cgx_handle *h, bool start) {
   const OpLearnedZ zop{h->r32, h->C32, L->z32, h->p32, L->eps, start ? 1 : 0,
                        ticket(h, kTicketInnerStart)};
   cudaError_t e;
-  if (h->compact16) {
-    CrsView<__nv_bfloat16, int16_t> GT{L->tptr, L->tcol16, L->gtsb, h->N, h->tile_cap};
-    CrsView<__nv_bfloat16, int16_t> Gv{L->gptr, L->gcol16, L->gsb, h->N, h->tile_cap};
-    e = launch_crs_view(h, GT, h->r32, OpInnerStore{L->y32});
-    if (e != cudaSuccess) return e;
-    return launch_crs_view(h, Gv, L->y32, zop);
+  if (L->sell_ok) {
+    const int nsl = (h->N + 31) / 32;
+    const int grid = std::max(1, std::min(h->num_sms * 8, (nsl + kWarps - 1) / kWarps));
+    k_sell<OpInnerStore><<<grid, kThreads, 0, h->stream>>>(
+        SellView{L->st_ptr, L->st_col, L->st_val, h->N}, h->r32,
+        OpInnerStore{L->y32}, h->st, h->partials);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    k_sell<OpLearnedZ><<<grid, kThreads, 0, h->stream>>>(
+        SellView{L->sg_ptr, L->sg_col, L->sg_val, h->N}, L->y32, zop, h->st,
+        h->partials);
+    return cudaGetLastError();
   }
   CrsView<float, int> GT{L->tptr, L->tcol, L->gts, h->N, h->tile_cap};
   CrsView<float, int> Gv{L->gptr, L->gcol, L->gs, h->N, h->tile_cap};
@@ -1486,8 +1496,9 @@ cgx_status learned_alloc(cgx_handle *h, int nnzL) {
   size_t o_t2g = take_n<int>(c, nnzL), o_g2t = take_n<int>(c, nnzL);
   size_t o_ghat = take_n<float>(c, nnzL), o_gs = take_n<float>(c, nnzL);
   size_t o_gts = take_n<float>(c, nnzL);
-  size_t o_gsb = take_n<__nv_bfloat16>(c, nnzL), o_gtsb = take_n<__nv_bfloat16>(c, nnzL);
-  size_t o_gc16 = take_n<int16_t>(c, nnzL), o_tc16 = take_n<int16_t>(c, nnzL);
+  const size_t nsl = (size_t)(N + 31) / 32;
+  size_t o_sgp = take_n<int>(c, nsl + 1), o_stp = take_n<int>(c, nsl + 1);
+  size_t o_g2sg = take_n<int>(c, nnzL), o_t2st = take_n<int>(c, nnzL);
   size_t o_h[4];
   for (int k = 0; k < 4; k++) o_h[k] = take_n<__nv_bfloat16>(c, (size_t)N * W);
   size_t o_o = take_n<float>(c, (size_t)N * NOUT);
@@ -1514,10 +1525,10 @@ cgx_status learned_alloc(cgx_handle *h, int nnzL) {
   L->ghat = (float *)(b + o_ghat);
   L->gs = (float *)(b + o_gs);
   L->gts = (float *)(b + o_gts);
-  L->gsb = (__nv_bfloat16 *)(b + o_gsb);
-  L->gtsb = (__nv_bfloat16 *)(b + o_gtsb);
-  L->gcol16 = (int16_t *)(b + o_gc16);
-  L->tcol16 = (int16_t *)(b + o_tc16);
+  L->sg_ptr = (int *)(b + o_sgp);
+  L->st_ptr = (int *)(b + o_stp);
+  L->g2sg = (int *)(b + o_g2sg);
+  L->t2st = (int *)(b + o_t2st);
   for (int k = 0; k < 4; k++) L->h[k] = (__nv_bfloat16 *)(b + o_h[k]);
   L->o = (float *)(b + o_o);
   L->y32 = (float *)(b + o_y);
@@ -1570,6 +1581,60 @@ cgx_status learned_train_alloc(cgx_handle *h) {
   return CGX_SUCCESS;
 }
 
+// SELL-32 layouts of G and G^T (see k_sell) when all their column offsets
+// fit in 16 bits; the slot maps let k_assemble write the values in place.
+cgx_status build_sell(cgx_handle *h) {
+  Learned *L = h->L;
+  const int N = h->N;
+  const int nsl = (N + 31) / 32;
+  cudaStream_t s = h->stream;
+  int *f16 = L->flag + 1;
+  int16_t *probe = nullptr;
+  // Fit check of every offset (|col - row| <= 32767) on the G and G^T
+  // patterns, into a scratch column array.
+  CUDA_TRY(cudaMalloc(&probe, sizeof(int16_t) * ((size_t)L->nnzL + kPad)));
+  CUDA_TRY(cudaMemsetAsync(f16, 0, sizeof(int), s));
+  k_delta16<<<grid_stream(h, N), kThreads, 0, s>>>(N, L->gptr, L->gcol, probe, f16);
+  k_delta16<<<grid_stream(h, N), kThreads, 0, s>>>(N, L->tptr, L->tcol, probe, f16);
+  CUDA_TRY(cudaGetLastError());
+  int fits = 0;
+  CUDA_TRY(cudaMemcpyAsync(&fits, f16, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  cudaFree(probe);
+  L->sell_ok = false;
+  if (fits != 0) return CGX_SUCCESS;
+  // Slice offsets: counts, then the exclusive scan.
+  int *cnt = nullptr;
+  CUDA_TRY(cudaMalloc(&cnt, sizeof(int) * ((size_t)nsl + kPad)));
+  int tot[2] = {0, 0};
+  k_sell_count<<<grid_stream(h, nsl), kThreads, 0, s>>>(N, L->gptr, cnt);
+  CUDA_TRY(scan(h, nsl, cnt, L->sg_ptr, L->sums));
+  CUDA_TRY(cudaMemcpyAsync(&tot[0], L->sg_ptr + nsl, sizeof(int), cudaMemcpyDeviceToHost, s));
+  k_sell_count<<<grid_stream(h, nsl), kThreads, 0, s>>>(N, L->tptr, cnt);
+  CUDA_TRY(scan(h, nsl, cnt, L->st_ptr, L->sums));
+  CUDA_TRY(cudaMemcpyAsync(&tot[1], L->st_ptr + nsl, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  cudaFree(cnt);
+  Carver c;
+  size_t o_gc = take_n<int16_t>(c, tot[0]), o_gv = take_n<__nv_bfloat16>(c, tot[0]);
+  size_t o_tc = take_n<int16_t>(c, tot[1]), o_tv = take_n<__nv_bfloat16>(c, tot[1]);
+  if (L->sell_mem) cudaFree(L->sell_mem);
+  CUDA_TRY(cudaMalloc(&L->sell_mem, c.off));
+  CUDA_TRY(cudaMemsetAsync(L->sell_mem, 0, c.off, s));
+  char *b = (char *)L->sell_mem;
+  L->sg_col = (int16_t *)(b + o_gc);
+  L->sg_val = (__nv_bfloat16 *)(b + o_gv);
+  L->st_col = (int16_t *)(b + o_tc);
+  L->st_val = (__nv_bfloat16 *)(b + o_tv);
+  k_sell_fill<<<grid_stream(h, N), kThreads, 0, s>>>(N, L->gptr, L->gcol, L->sg_ptr,
+                                                     L->sg_col, L->g2sg);
+  k_sell_fill<<<grid_stream(h, N), kThreads, 0, s>>>(N, L->tptr, L->tcol, L->st_ptr,
+                                                     L->st_col, L->t2st);
+  CUDA_TRY(cudaGetLastError());
+  L->sell_ok = true;
+  return CGX_SUCCESS;
+}
+
 // Forward pass of the network on h's scaled graph; writes Ghat (and the
 // scaled G, G^T for the apply when `scaled`).
 cudaError_t gnn_forward(cgx_handle *h, const float *P, bool scaled) {
@@ -1589,11 +1654,12 @@ cudaError_t gnn_forward(cgx_handle *h, const float *P, bool scaled) {
                                                l, L->h[l], L->h[l + 1],
                                                keep ? L->agg[l] : nullptr,
                                                keep ? L->pre[l + 1] : nullptr);
-  k_head<<<grid_for(h, (size_t)N * NOUT), kThreads, 0, s>>>(N, L->h[3], P, L->o);
+  k_head<<<grid_for(h, (size_t)N), kThreads, 0, s>>>(N, L->h[3], P, L->o);
   k_assemble<<<grid_for(h, L->nnzL), kThreads, 0, s>>>(
       L->nnzL, L->grow, L->gcol, L->g2a, L->ahat, L->o, L->ghat, L->dis,
       L->g2t, scaled ? L->gs : nullptr, scaled ? L->gts : nullptr,
-      scaled ? L->gsb : nullptr, scaled ? L->gtsb : nullptr);
+      scaled && L->sell_ok ? L->sg_val : nullptr,
+      scaled && L->sell_ok ? L->st_val : nullptr, L->g2sg, L->t2st);
   return cudaGetLastError();
 }
 
@@ -1842,14 +1908,7 @@ cgx_status cgx_learned_setup(cgx_handle *h) {
   k_transpose_map<<<grid_stream(h, L->nnzL), kThreads, 0, s>>>(
       L->nnzL, L->grow, L->gcol, L->tptr, L->tcol, L->g2t, L->t2g, L->flag);
   CUDA_TRY(cudaGetLastError());
-  {
-    // 16-bit column offsets of G and G^T (used when A's fit, see ensure_f32).
-    int *f16 = L->flag + 1;
-    CUDA_TRY(cudaMemsetAsync(f16, 0, sizeof(int), s));
-    k_delta16<<<g, kThreads, 0, s>>>(N, L->gptr, L->gcol, L->gcol16, f16);
-    k_delta16<<<g, kThreads, 0, s>>>(N, L->tptr, L->tcol, L->tcol16, f16);
-    CUDA_TRY(cudaGetLastError());
-  }
+  CGX_TRY(build_sell(h));
   CUDA_TRY(cudaMemcpyAsync(h->host_scalar, L->flag, sizeof(int),
                            cudaMemcpyDeviceToHost, s));
   CUDA_TRY(cudaStreamSynchronize(s));

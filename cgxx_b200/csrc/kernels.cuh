@@ -216,15 +216,18 @@ __global__ void __launch_bounds__(kThreads)
     const int r1 = min(N, r0 + kThreads);
     const int s = __ldg(&A.ptr[r0]), e = __ldg(&A.ptr[r1]);
     const bool staged = cap > 0 && e > s && e - s <= cap;
+    // The row bounds are loaded before the wait so that their latency
+    // overlaps the bulk copy's.
+    const int row = r0 + threadIdx.x;
+    const int j0 = row < r1 ? __ldg(&A.ptr[row]) : 0;
+    const int j1 = row < r1 ? __ldg(&A.ptr[row + 1]) : 0;
     bool ok = true;
     if (staged) {
       ok = mbar_wait_bounded(&bars[buf], buf ? ph1 : ph0);
       if (buf) ph1 ^= 1u; else ph0 ^= 1u;
       if (!ok && threadIdx.x == 0) atomicOr(&st->error, kErrBarrierTimeout);
     }
-    const int row = r0 + threadIdx.x;
     if (row < r1) {
-      const int j0 = __ldg(&A.ptr[row]), j1 = __ldg(&A.ptr[row + 1]);
       XT sum = 0;
       if (staged) {
         if (ok) {
@@ -239,6 +242,76 @@ __global__ void __launch_bounds__(kThreads)
       op.row(row, sum, acc);
     }
     __syncthreads();
+  }
+  op.finish(acc, st, partials);
+}
+
+// ---------------------------------------------------------------------------
+// Sliced ELL (SELL-32) SpMV for short rows (the learned factor G and G^T, ~4
+// entries per row on a 7-point matrix). Rows are taken in order in slices of
+// 32; slice s holds width(s) = max row length of its rows, stored column-major
+// from sptr[s]: entry k of row s*32 + r at sptr[s] + 32 k + r. Values are
+// BF16, columns 16-bit offsets from the row; padding slots hold value 0 and
+// offset 0. A warp owns a slice (lane = row), so every value/offset load is
+// one coalesced 64-byte access, no row pointers are read, and four gathers
+// per lane are in flight.
+struct SellView {
+  const int *sptr;  // nslices + 1 element offsets
+  const int16_t *col;
+  const __nv_bfloat16 *val;
+  int N;
+};
+
+template <typename Op>
+__global__ void __launch_bounds__(kThreads)
+    k_sell(SellView A, const float *__restrict__ x, Op op, CgState *st,
+           double *partials) {
+  if (op.skip(st)) return;
+  typename Op::Acc acc;
+  constexpr int SPW = 2;  // slices a warp works on at once
+  const int lane = threadIdx.x & 31;
+  const int nslices = (A.N + 31) >> 5;
+  const int warp = (blockIdx.x * kThreads + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * kThreads) >> 5;
+  for (int s0 = warp * SPW; s0 < nslices; s0 += nwarps * SPW) {
+    int b[SPW], w[SPW];
+#pragma unroll
+    for (int q = 0; q < SPW; q++) {
+      const int s = min(s0 + q, nslices - 1);
+      b[q] = __ldg(&A.sptr[s]);
+      w[q] = s0 + q < nslices ? (__ldg(&A.sptr[s + 1]) - b[q]) >> 5 : 0;
+    }
+    int wmax = 0;
+#pragma unroll
+    for (int q = 0; q < SPW; q++) wmax = max(wmax, w[q]);
+    float sum[SPW];
+#pragma unroll
+    for (int q = 0; q < SPW; q++) sum[q] = 0.f;
+    for (int k = 0; k < wmax; k += 4) {
+      float xv[SPW][4], vv[SPW][4];
+#pragma unroll
+      for (int q = 0; q < SPW; q++) {
+        const int rr = min(((s0 + q) << 5) + lane, A.N - 1);  // padding lanes: row N-1
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          if (k + u < w[q]) {
+            const int slot = b[q] + ((k + u) << 5) + lane;
+            vv[q][u] = __bfloat162float(A.val[slot]);
+            xv[q][u] = __ldg(&x[rr + (int)A.col[slot]]);
+          }
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < SPW; q++)
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+          if (k + u < w[q]) sum[q] = fmaf(vv[q][u], xv[q][u], sum[q]);
+    }
+#pragma unroll
+    for (int q = 0; q < SPW; q++) {
+      const int row = ((s0 + q) << 5) + lane;
+      if (s0 + q < nslices && row < A.N) op.row(row, sum[q], acc);
+    }
   }
   op.finish(acc, st, partials);
 }
@@ -838,7 +911,24 @@ __global__ void __launch_bounds__(kThreads)
   if (st->in_stop) return;
   const float na = (float)(-st->in_alpha);
   double rr = 0.0;
-  for (int i = blockIdx.x * kThreads + threadIdx.x; i < N;
+  const int n4 = N >> 2;
+  float4 *r4 = reinterpret_cast<float4 *>(r);
+  const float4 *q4 = reinterpret_cast<const float4 *>(q);
+  for (int i = blockIdx.x * kThreads + threadIdx.x; i < n4;
+       i += gridDim.x * kThreads) {
+    float4 rv = r4[i];
+    const float4 qv = __ldg(&q4[i]);
+    rv.x = fmaf(na, qv.x, rv.x);
+    rv.y = fmaf(na, qv.y, rv.y);
+    rv.z = fmaf(na, qv.z, rv.z);
+    rv.w = fmaf(na, qv.w, rv.w);
+    r4[i] = rv;
+    rr = fma((double)rv.x, (double)rv.x, rr);
+    rr = fma((double)rv.y, (double)rv.y, rr);
+    rr = fma((double)rv.z, (double)rv.z, rr);
+    rr = fma((double)rv.w, (double)rv.w, rr);
+  }
+  for (int i = 4 * n4 + blockIdx.x * kThreads + threadIdx.x; i < N;
        i += gridDim.x * kThreads) {
     const float ri = fmaf(na, q[i], r[i]);
     r[i] = ri;
@@ -865,7 +955,26 @@ __global__ void __launch_bounds__(kThreads)
   if (st->in_finished) return;
   const float a = (float)st->in_alpha, b = (float)st->in_beta;
   const bool upd = !st->in_stop;
-  for (int i = blockIdx.x * kThreads + threadIdx.x; i < N;
+  const int n4 = N >> 2;
+  float4 *d4 = reinterpret_cast<float4 *>(d);
+  float4 *p4 = reinterpret_cast<float4 *>(p);
+  const float4 *z4 = reinterpret_cast<const float4 *>(z);
+  for (int i = blockIdx.x * kThreads + threadIdx.x; i < n4;
+       i += gridDim.x * kThreads) {
+    const float4 pv = p4[i];
+    float4 dv = d4[i];
+    dv.x = fmaf(a, pv.x, dv.x);
+    dv.y = fmaf(a, pv.y, dv.y);
+    dv.z = fmaf(a, pv.z, dv.z);
+    dv.w = fmaf(a, pv.w, dv.w);
+    d4[i] = dv;
+    if (upd) {
+      const float4 zv = __ldg(&z4[i]);
+      p4[i] = make_float4(fmaf(b, pv.x, zv.x), fmaf(b, pv.y, zv.y),
+                          fmaf(b, pv.z, zv.z), fmaf(b, pv.w, zv.w));
+    }
+  }
+  for (int i = 4 * n4 + blockIdx.x * kThreads + threadIdx.x; i < N;
        i += gridDim.x * kThreads) {
     const float pv = p[i];
     d[i] = fmaf(a, pv, d[i]);

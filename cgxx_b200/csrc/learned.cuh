@@ -253,8 +253,8 @@ __global__ void __launch_bounds__(32 * kLayerWarps)
             int layer, const __nv_bfloat16 *__restrict__ hin,
             __nv_bfloat16 *__restrict__ hout, __nv_bfloat16 *__restrict__ agg_out,
             float *__restrict__ pre_out) {
-  __shared__ __nv_bfloat16 sW[W][2 * W];           // W_l[n][k]
-  __shared__ __nv_bfloat16 sX[kLayerWarps][16][2 * W + 8];  // padded rows
+  __shared__ __align__(16) __nv_bfloat16 sW[W][2 * W + 8];  // W_l[n][k], rows padded (banks)
+  __shared__ __align__(16) __nv_bfloat16 sX[kLayerWarps][16][2 * W + 8];  // padded rows
   __shared__ float sB[W];
   const float *Wl = P + OFF_L0 + layer * L_STRIDE;
   for (int t = threadIdx.x; t < W * 2 * W; t += blockDim.x)
@@ -268,24 +268,53 @@ __global__ void __launch_bounds__(32 * kLayerWarps)
   for (int grp = blockIdx.x * kLayerWarps + warp; grp < groups;
        grp += gridDim.x * kLayerWarps) {
     const int base = grp * 16;
-    // Gather.
-    for (int r = 0; r < 16; r++) {
+    // Gather: the warp's 16 nodes x 4 chunks of 8 features are 64 tasks,
+    // two per lane, so all 16 nodes' neighbour rows are in flight at once;
+    // a task reads 16 bytes (8 BF16 features) per neighbour, up to 4
+    // neighbours requested before they are summed (in entry order).
+    const uint4 *hin4 = reinterpret_cast<const uint4 *>(hin);
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+      const int task = lane + 32 * q;
+      const int r = task >> 2, c4 = task & 3;
       const int i = base + r;
-      float a = 0.f;
-      __nv_bfloat16 hs = __float2bfloat16_rn(0.f);
+      float a[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+      uint4 own = make_uint4(0u, 0u, 0u, 0u);
       if (i < N) {
-        hs = hin[(size_t)i * W + lane];
-        for (int j = ptr[i]; j < ptr[i + 1]; j++) {
-          const int c = index[j];
-          if (c != i)
-            a = fmaf(fabsf(ahat[j]),
-                     __bfloat162float(hin[(size_t)c * W + lane]), a);
+        own = hin4[(size_t)i * (W / 8) + c4];
+        const int j0 = ptr[i], j1 = ptr[i + 1];
+        for (int j = j0; j < j1; j += 4) {
+          float w[4];
+          uint4 hv[4];
+#pragma unroll
+          for (int u = 0; u < 4; u++) {
+            if (j + u < j1) {
+              const int c = index[j + u];
+              w[u] = c != i ? fabsf(ahat[j + u]) : 0.f;
+              hv[u] = hin4[(size_t)c * (W / 8) + c4];
+            }
+          }
+#pragma unroll
+          for (int u = 0; u < 4; u++) {
+            if (j + u < j1) {
+              const __nv_bfloat162 *b2 = reinterpret_cast<const __nv_bfloat162 *>(&hv[u]);
+#pragma unroll
+              for (int k = 0; k < 4; k++) {
+                a[2 * k] = fmaf(w[u], __low2float(b2[k]), a[2 * k]);
+                a[2 * k + 1] = fmaf(w[u], __high2float(b2[k]), a[2 * k + 1]);
+              }
+            }
+          }
         }
       }
-      const __nv_bfloat16 ab = __float2bfloat16_rn(a);
-      sX[warp][r][lane] = hs;
-      sX[warp][r][W + lane] = ab;
-      if (agg_out && i < N) agg_out[(size_t)i * W + lane] = ab;
+      uint4 ag;
+      __nv_bfloat162 *ag2 = reinterpret_cast<__nv_bfloat162 *>(&ag);
+#pragma unroll
+      for (int k = 0; k < 4; k++) ag2[k] = __floats2bfloat162_rn(a[2 * k], a[2 * k + 1]);
+      *reinterpret_cast<uint4 *>(&sX[warp][r][8 * c4]) = own;
+      *reinterpret_cast<uint4 *>(&sX[warp][r][W + 8 * c4]) = ag;
+      if (agg_out && i < N)
+        reinterpret_cast<uint4 *>(agg_out)[(size_t)i * (W / 8) + c4] = ag;
     }
     __syncwarp();
     // pre = X W^T on the tensor cores.
@@ -331,18 +360,35 @@ __global__ void __launch_bounds__(32 * kLayerWarps)
   }
 }
 
-// o_i = W_h h_i + b_h (FP32): per node, NOUT outputs.
+// o_i = W_h h_i + b_h (FP32): one thread per node, its 32 features loaded
+// once (four 16-byte loads), W_h from shared memory.
 __global__ void k_head(int N, const __nv_bfloat16 *__restrict__ h,
                        const float *__restrict__ P, float *__restrict__ o) {
-  const int total = N * NOUT;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total;
-       t += gridDim.x * blockDim.x) {
-    const int i = t / NOUT, k = t % NOUT;
-    float s = P[OFF_BH + k];
-#pragma unroll 8
-    for (int f = 0; f < W; f++)
-      s = fmaf(P[OFF_WH + k * W + f], __bfloat162float(h[(size_t)i * W + f]), s);
-    o[t] = s;
+  __shared__ float sW[NOUT * W + NOUT];
+  for (int t = threadIdx.x; t < NOUT * W + NOUT; t += blockDim.x)
+    sW[t] = P[OFF_WH + t];
+  __syncthreads();
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N;
+       i += gridDim.x * blockDim.x) {
+    float hv[W];
+    const uint4 *src = reinterpret_cast<const uint4 *>(h + (size_t)i * W);
+#pragma unroll
+    for (int q = 0; q < W / 8; q++) {
+      const uint4 u = src[q];
+      const __nv_bfloat162 *b2 = reinterpret_cast<const __nv_bfloat162 *>(&u);
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        hv[q * 8 + 2 * k] = __low2float(b2[k]);
+        hv[q * 8 + 2 * k + 1] = __high2float(b2[k]);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < NOUT; k++) {
+      float s = sW[NOUT * W + k];
+#pragma unroll
+      for (int f = 0; f < W; f++) s = fmaf(sW[k * W + f], hv[f], s);
+      o[(size_t)i * NOUT + k] = s;
+    }
   }
 }
 
@@ -355,8 +401,10 @@ __global__ void k_assemble(int nnzL, const int *__restrict__ grow,
                            const float *__restrict__ o, float *__restrict__ ghat,
                            const double *__restrict__ dis,
                            const int *__restrict__ g2t, float *__restrict__ gs,
-                           float *__restrict__ gts, __nv_bfloat16 *__restrict__ gsb,
-                           __nv_bfloat16 *__restrict__ gtsb) {
+                           float *__restrict__ gts, __nv_bfloat16 *__restrict__ sgv,
+                           __nv_bfloat16 *__restrict__ stv,
+                           const int *__restrict__ g2sg,
+                           const int *__restrict__ t2st) {
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nnzL;
        e += gridDim.x * blockDim.x) {
     const int i = grow[e], j = gcol[e];
@@ -375,10 +423,10 @@ __global__ void k_assemble(int nnzL, const int *__restrict__ grow,
       const float sv = (float)(dis[i] * (double)v);
       gs[e] = sv;
       gts[g2t[e]] = sv;
-      if (gsb) {
+      if (sgv) {
         const __nv_bfloat16 bv = __float2bfloat16_rn(sv);
-        gsb[e] = bv;
-        gtsb[g2t[e]] = bv;
+        sgv[g2sg[e]] = bv;
+        stv[t2st[g2t[e]]] = bv;
       }
     }
   }
@@ -710,6 +758,36 @@ __global__ void k_adam(int n, float *__restrict__ p, float *__restrict__ m,
     m[k] = mk;
     v[k] = vk;
     p[k] -= lr * (mk / c1) / (sqrtf(vk / c2) + eps);
+  }
+}
+
+// SELL-32 build from a CRS pattern: slot count 32 * (max row length) per
+// slice (written to cnt[s] for the scan that gives the slice offsets).
+__global__ void k_sell_count(int N, const int *__restrict__ rp, int *cnt) {
+  const int nslices = (N + 31) >> 5;
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nslices;
+       s += gridDim.x * blockDim.x) {
+    int w = 0;
+    for (int r = s * 32; r < min(N, s * 32 + 32); r++)
+      w = max(w, rp[r + 1] - rp[r]);
+    cnt[s] = 32 * w;
+  }
+}
+
+// SELL-32 slot of every CRS entry (map) and its 16-bit column offset; the
+// padding slots keep the zero value / zero offset they were cleared to.
+__global__ void k_sell_fill(int N, const int *__restrict__ rp,
+                            const int *__restrict__ col,
+                            const int *__restrict__ sptr,
+                            int16_t *__restrict__ scol, int *__restrict__ map) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N;
+       i += gridDim.x * blockDim.x) {
+    const int base = sptr[i >> 5] + (i & 31);
+    for (int k = 0; k < rp[i + 1] - rp[i]; k++) {
+      const int e = rp[i] + k, dst = base + (k << 5);
+      scol[dst] = (int16_t)(col[e] - i);
+      map[e] = dst;
+    }
   }
 }
 
