@@ -414,7 +414,7 @@ def our_arm(args, world, rank, local):
                    "launches": r["spmv_launches"]}
     peak, peak_kind = peaks()
     fp64_spmv_bytes = 12 * nnz + 4 * (N + 1) + 16 * N  # values+cols, ptr, p once, q
-    fp32_spmv_bytes = 8 * nnz + 4 * (N + 1) + 8 * N
+    fp32_spmv_bytes = 8 * nnz + 4 * (N + 1) + 8 * N  # FP32 CRS
     plain_iter_bytes = fp64_spmv_bytes + 32 * N + 48 * N
     kp = kern["plain"]
     plain_iter_us = kp["spmv_us"] + kp["update_us"] + kp["direction_us"]
@@ -429,12 +429,20 @@ def our_arm(args, world, rank, local):
         roof = fp64_roof
     else:
         kk = kern[args.path]
+        slots, uniform, slices = h.inner_layout()
+        if slots:
+            # SELL-U: FP32 values, 16-byte slice descriptors, p once, q
+            # written (a uniform slice carries no per-entry index).
+            fp32_spmv_bytes = 4 * nnz + 16 * slices + 8 * N
+            kname = (f"k_sellu<float, OpInnerQ>: q = A p fused with <p,q> (FP32 SELL-U, "
+                     f"{uniform}/{slices} slices uniform, {slots} value slots)")
+        else:
+            kname = "k_crs<float, OpInnerQ>: q = A p fused with <p,q> (FP32 CRS, inner)"
         roof = {"bound": "hbm", "achieved": fp32_spmv_bytes / (kk["spmv_us"] * 1e-6) / 1e9,
-                "peak": peak, "unit": "GB/s",
-                "kernel": "k_crs<float, OpInnerQ>: q = A p fused with <p,q> (FP32 CRS, inner)",
+                "peak": peak, "unit": "GB/s", "kernel": kname,
                 "algorithmic_bytes": fp32_spmv_bytes, "peak_kind": peak_kind}
         roof["frac"] = roof["achieved"] / peak
-        prof32 = read_traffic_profile("spmv_crs_fp32_diffusion7_160.json")
+        prof32 = read_traffic_profile("spmv_sellu_fp32_diffusion7_160.json")
         roof["traffic"] = prof32.get("dram_bytes_per_launch") if prof32 else None
 
     # End to end through the public C ABI: pinned host inputs uploaded every

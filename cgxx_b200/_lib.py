@@ -102,6 +102,8 @@ PROTOTYPES = {
     "cgx_apply_jacobi": [_P, _I, _I],
     "cgx_solve": [_P, C.POINTER(Options), C.POINTER(Result)],
     "cgx_true_residual": [_P, _PD],
+    "cgx_inner_layout": [_P, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),
+                         C.POINTER(C.c_longlong)],
     "cgx_mtx_read": [C.c_char_p, _PI, _PI, C.POINTER(_PI), C.POINTER(_PI),
                      C.POINTER(_PD)],
     "cgx_mtx_write_symmetric_crs": [C.c_char_p, _I, _P, _P, _P],
@@ -282,6 +284,13 @@ class Handle:
         r = C.c_double()
         check(self._lib.cgx_true_residual(self._h, C.byref(r)))
         return r.value
+
+    def inner_layout(self):
+        """(value_slots, uniform_slices, slices) of A's FP32 copy for the
+        inner SpMV; value_slots == 0 means FP32 CRS."""
+        a, b, c = C.c_longlong(), C.c_longlong(), C.c_longlong()
+        check(self._lib.cgx_inner_layout(self._h, C.byref(a), C.byref(b), C.byref(c)))
+        return a.value, b.value, c.value
 
     # --- learned preconditioner ---
     def update_crs_values(self, value):

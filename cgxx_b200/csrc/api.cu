@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -23,6 +24,7 @@
 #include "cgx.h"
 #include "kernels.cuh"
 #include "learned.cuh"
+#include "sell.cuh"
 
 using namespace cgx;
 
@@ -110,6 +112,24 @@ struct Carver {
 
 }  // namespace
 
+// SELL-U layout of a CRS pattern (sell.cuh): slice meta, offsets and the
+// value slot of every CRS entry (map); `slots` values including padding.
+struct SellU {
+  void *mem = nullptr;
+  int4 *meta = nullptr;
+  int *off = nullptr;
+  int *map = nullptr;
+  size_t slots = 0;
+  long long uniform = 0;  // slices with uniform offsets
+  int max_width = 0;      // largest slot count of a slice
+  bool ok = false;
+};
+
+static void sellu_free(SellU &S) {
+  if (S.mem) cudaFree(S.mem);
+  S = SellU{};
+}
+
 struct cgx_handle {
   int device = 0;
   int num_sms = 148;
@@ -148,6 +168,11 @@ struct cgx_handle {
   float *d32 = nullptr, *r32 = nullptr, *p32 = nullptr, *q32 = nullptr;
   double *r64 = nullptr;
   bool f32_valid = false;
+  // SELL-U copy of A's FP32 values for the inner SpMV (built with the FP32
+  // mirror; sa.ok when the layout's indices fit in int).
+  SellU sa;
+  float *sa_val = nullptr;
+  bool sa_tried = false;
 
   // Scratch: state, partial sums, dot result, validation flag.
   void *scratch = nullptr;
@@ -176,13 +201,12 @@ struct Learned {
   int *gptr = nullptr, *gcol = nullptr, *grow = nullptr, *g2a = nullptr;
   int *tptr = nullptr, *tcol = nullptr, *t2g = nullptr, *g2t = nullptr;
   float *ghat = nullptr, *gs = nullptr, *gts = nullptr;
-  // SELL-32 copies of G and G^T for the apply (BF16 values, 16-bit column
-  // offsets), used when every offset fits (sell_ok).
-  void *sell_mem = nullptr;
-  bool sell_ok = false;
-  int *sg_ptr = nullptr, *st_ptr = nullptr, *g2sg = nullptr, *t2st = nullptr;
-  int16_t *sg_col = nullptr, *st_col = nullptr;
+  // SELL-U copies of G and G^T for the apply (BF16 values), used when both
+  // layouts were built (sell_ok); their maps take the values from k_assemble.
+  SellU sg, st;
+  void *sell_val = nullptr;
   __nv_bfloat16 *sg_val = nullptr, *st_val = nullptr;
+  bool sell_ok = false;
   __nv_bfloat16 *h[4] = {};
   __nv_bfloat16 *agg[3] = {};
   float *pre[4] = {};
@@ -218,7 +242,9 @@ static void free_learned(cgx_handle *h) {
   if (!h->L) return;
   if (h->L->mem) cudaFree(h->L->mem);
   if (h->L->train) cudaFree(h->L->train);
-  if (h->L->sell_mem) cudaFree(h->L->sell_mem);
+  sellu_free(h->L->sg);
+  sellu_free(h->L->st);
+  if (h->L->sell_val) cudaFree(h->L->sell_val);
   delete h->L;
   h->L = nullptr;
 }
@@ -230,6 +256,10 @@ static void free_matrix(cgx_handle *h) {
   if (h->vec_mem) cudaFree(h->vec_mem);
   if (h->f32_mem) cudaFree(h->f32_mem);
   h->mat_mem = h->vec_mem = h->f32_mem = nullptr;
+  sellu_free(h->sa);
+  if (h->sa_val) cudaFree(h->sa_val);
+  h->sa_val = nullptr;
+  h->sa_tried = false;
   h->format = -1;
   h->N = h->nz = 0;
   h->ptr = h->index = nullptr;
@@ -412,8 +442,35 @@ static cudaError_t launch_pcg_setup(cgx_handle *h, bool jacobi) {
 }
 
 // q = A p in FP32 with <p,q> (inner solves), compact indices when they fit.
+// k_sellu over one wave of CTAs (as many as fit on the SMs at once), fewer
+// when the slice pairs run out; chunks of 4 slots when no slice is wider.
+template <typename VT, int U, typename Op>
+static cudaError_t launch_sellu_u(cgx_handle *h, SellUView<VT> A, const float *x,
+                                  Op op) {
+  auto kern = k_sellu<VT, U, Op>;
+  int per_sm = 0;
+  cudaError_t e =
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, 0);
+  if (e != cudaSuccess) return e;
+  const int pairs = ((h->N + 31) / 32 + 1) / 2;
+  const int grid = std::max(1, std::min(h->num_sms * std::max(1, per_sm),
+                                        (pairs + kWarps - 1) / kWarps));
+  kern<<<grid, kThreads, 0, h->stream>>>(A, x, op, h->st, h->partials);
+  return cudaGetLastError();
+}
+
+template <typename VT, typename Op>
+static cudaError_t launch_sellu(cgx_handle *h, const SellU &S, const VT *val,
+                                const float *x, Op op) {
+  const SellUView<VT> A{S.meta, S.off, val, h->N};
+  return S.max_width <= 4 ? launch_sellu_u<VT, 4>(h, A, x, op)
+                          : launch_sellu_u<VT, 8>(h, A, x, op);
+}
+
 static cudaError_t launch_inner_q(cgx_handle *h) {
   OpInnerQ op{h->p32, h->q32, ticket(h, kTicketInnerQ)};
+  if (h->sa.ok)
+    return launch_sellu(h, h->sa, h->sa_val, h->p32, op);
   if (h->compact16)
     return launch_crs_view(
         h, CrsView<float, int16_t>{h->ptr, h->idx16, h->value32, h->N, h->tile_cap},
@@ -722,6 +779,16 @@ cgx_status cgx_host_alloc(void **p, size_t bytes) {
 
 cgx_status cgx_host_free(void *p) {
   if (p) CUDA_TRY(cudaFreeHost(p));
+  return CGX_SUCCESS;
+}
+
+cgx_status cgx_inner_layout(cgx_handle *h, long long *value_slots,
+                            long long *uniform_slices, long long *slices) {
+  if (!h) return fail(CGX_ERROR_INVALID_ARGUMENT, "handle is NULL");
+  const bool ok = h->sa.ok;
+  if (value_slots) *value_slots = ok ? (long long)h->sa.slots : 0;
+  if (uniform_slices) *uniform_slices = ok ? h->sa.uniform : 0;
+  if (slices) *slices = ok ? (h->N + 31) / 32 : 0;
   return CGX_SUCCESS;
 }
 
@@ -1176,6 +1243,11 @@ static cgx_status solve_fp64(cgx_handle *h, const cgx_options &o,
   return CGX_SUCCESS;
 }
 
+namespace {
+cgx_status build_sellu(cgx_handle *h, const int *ptr, const int *col,
+                       size_t nnz, SellU &S);
+}
+
 static cgx_status ensure_f32(cgx_handle *h) {
   if (h->f32_valid) return CGX_SUCCESS;
   const int N = h->N;
@@ -1207,6 +1279,21 @@ static cgx_status ensure_f32(cgx_handle *h) {
   k_to_f32<<<grid_stream(h, N), kThreads, 0, h->stream>>>((size_t)N, h->C,
                                                           h->C32);
   CUDA_TRY(cudaGetLastError());
+  // SELL-U copy of A (pattern once per matrix, values on every refresh).
+  if (!h->sa_tried) {
+    h->sa_tried = true;
+    CGX_TRY(build_sellu(h, h->ptr, h->index, (size_t)h->nz, h->sa));
+    if (h->sa.ok) {
+      CUDA_TRY(cudaMalloc(&h->sa_val, sizeof(float) * (h->sa.slots + kPad)));
+      CUDA_TRY(cudaMemsetAsync(h->sa_val, 0, sizeof(float) * (h->sa.slots + kPad),
+                               h->stream));
+    }
+  }
+  if (h->sa.ok) {
+    k_sellu_scatter<double, float><<<grid_stream(h, h->nz), kThreads, 0, h->stream>>>(
+        (size_t)h->nz, h->sa.map, h->value, h->sa_val);
+    CUDA_TRY(cudaGetLastError());
+  }
   CUDA_TRY(cudaMemsetAsync(h->flag, 0, sizeof(int), h->stream));
   k_delta16<<<grid_stream(h, N), kThreads, 0, h->stream>>>(N, h->ptr, h->index,
                                                            h->idx16, h->flag);
@@ -1239,16 +1326,9 @@ static cudaError_t launch_learned_apply(cgx_handle *h, bool start) {
                        ticket(h, kTicketInnerStart)};
   cudaError_t e;
   if (L->sell_ok) {
-    const int nsl = (h->N + 31) / 32;
-    const int grid = std::max(1, std::min(h->num_sms * 8, (nsl + kWarps - 1) / kWarps));
-    k_sell<OpInnerStore><<<grid, kThreads, 0, h->stream>>>(
-        SellView{L->st_ptr, L->st_col, L->st_val, h->N}, h->r32,
-        OpInnerStore{L->y32}, h->st, h->partials);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    k_sell<OpLearnedZ><<<grid, kThreads, 0, h->stream>>>(
-        SellView{L->sg_ptr, L->sg_col, L->sg_val, h->N}, L->y32, zop, h->st,
-        h->partials);
-    return cudaGetLastError();
+    e = launch_sellu(h, L->st, L->st_val, h->r32, OpInnerStore{L->y32});
+    if (e != cudaSuccess) return e;
+    return launch_sellu(h, L->sg, L->sg_val, L->y32, zop);
   }
   CrsView<float, int> GT{L->tptr, L->tcol, L->gts, h->N, h->tile_cap};
   CrsView<float, int> Gv{L->gptr, L->gcol, L->gs, h->N, h->tile_cap};
@@ -1496,9 +1576,6 @@ cgx_status learned_alloc(cgx_handle *h, int nnzL) {
   size_t o_t2g = take_n<int>(c, nnzL), o_g2t = take_n<int>(c, nnzL);
   size_t o_ghat = take_n<float>(c, nnzL), o_gs = take_n<float>(c, nnzL);
   size_t o_gts = take_n<float>(c, nnzL);
-  const size_t nsl = (size_t)(N + 31) / 32;
-  size_t o_sgp = take_n<int>(c, nsl + 1), o_stp = take_n<int>(c, nsl + 1);
-  size_t o_g2sg = take_n<int>(c, nnzL), o_t2st = take_n<int>(c, nnzL);
   size_t o_h[4];
   for (int k = 0; k < 4; k++) o_h[k] = take_n<__nv_bfloat16>(c, (size_t)N * W);
   size_t o_o = take_n<float>(c, (size_t)N * NOUT);
@@ -1525,10 +1602,6 @@ cgx_status learned_alloc(cgx_handle *h, int nnzL) {
   L->ghat = (float *)(b + o_ghat);
   L->gs = (float *)(b + o_gs);
   L->gts = (float *)(b + o_gts);
-  L->sg_ptr = (int *)(b + o_sgp);
-  L->st_ptr = (int *)(b + o_stp);
-  L->g2sg = (int *)(b + o_g2sg);
-  L->t2st = (int *)(b + o_t2st);
   for (int k = 0; k < 4; k++) L->h[k] = (__nv_bfloat16 *)(b + o_h[k]);
   L->o = (float *)(b + o_o);
   L->y32 = (float *)(b + o_y);
@@ -1581,56 +1654,89 @@ cgx_status learned_train_alloc(cgx_handle *h) {
   return CGX_SUCCESS;
 }
 
-// SELL-32 layouts of G and G^T (see k_sell) when all their column offsets
-// fit in 16 bits; the slot maps let k_assemble write the values in place.
-cgx_status build_sell(cgx_handle *h) {
-  Learned *L = h->L;
+// SELL-U layout of the CRS pattern (ptr, col) with nnz entries into S
+// (sell.cuh). S.ok stays false when its value slots or offsets would not fit
+// in int; the callers then keep their CRS kernels.
+cgx_status build_sellu(cgx_handle *h, const int *ptr, const int *col,
+                       size_t nnz, SellU &S) {
+  sellu_free(S);
   const int N = h->N;
   const int nsl = (N + 31) / 32;
   cudaStream_t s = h->stream;
-  int *f16 = L->flag + 1;
-  int16_t *probe = nullptr;
-  // Fit check of every offset (|col - row| <= 32767) on the G and G^T
-  // patterns, into a scratch column array.
-  CUDA_TRY(cudaMalloc(&probe, sizeof(int16_t) * ((size_t)L->nnzL + kPad)));
-  CUDA_TRY(cudaMemsetAsync(f16, 0, sizeof(int), s));
-  k_delta16<<<grid_stream(h, N), kThreads, 0, s>>>(N, L->gptr, L->gcol, probe, f16);
-  k_delta16<<<grid_stream(h, N), kThreads, 0, s>>>(N, L->tptr, L->tcol, probe, f16);
-  CUDA_TRY(cudaGetLastError());
-  int fits = 0;
-  CUDA_TRY(cudaMemcpyAsync(&fits, f16, sizeof(int), cudaMemcpyDeviceToHost, s));
-  CUDA_TRY(cudaStreamSynchronize(s));
-  cudaFree(probe);
-  L->sell_ok = false;
-  if (fits != 0) return CGX_SUCCESS;
-  // Slice offsets: counts, then the exclusive scan.
-  int *cnt = nullptr;
-  CUDA_TRY(cudaMalloc(&cnt, sizeof(int) * ((size_t)nsl + kPad)));
-  int tot[2] = {0, 0};
-  k_sell_count<<<grid_stream(h, nsl), kThreads, 0, s>>>(N, L->gptr, cnt);
-  CUDA_TRY(scan(h, nsl, cnt, L->sg_ptr, L->sums));
-  CUDA_TRY(cudaMemcpyAsync(&tot[0], L->sg_ptr + nsl, sizeof(int), cudaMemcpyDeviceToHost, s));
-  k_sell_count<<<grid_stream(h, nsl), kThreads, 0, s>>>(N, L->tptr, cnt);
-  CUDA_TRY(scan(h, nsl, cnt, L->st_ptr, L->sums));
-  CUDA_TRY(cudaMemcpyAsync(&tot[1], L->st_ptr + nsl, sizeof(int), cudaMemcpyDeviceToHost, s));
-  CUDA_TRY(cudaStreamSynchronize(s));
-  cudaFree(cnt);
   Carver c;
-  size_t o_gc = take_n<int16_t>(c, tot[0]), o_gv = take_n<__nv_bfloat16>(c, tot[0]);
-  size_t o_tc = take_n<int16_t>(c, tot[1]), o_tv = take_n<__nv_bfloat16>(c, tot[1]);
-  if (L->sell_mem) cudaFree(L->sell_mem);
-  CUDA_TRY(cudaMalloc(&L->sell_mem, c.off));
-  CUDA_TRY(cudaMemsetAsync(L->sell_mem, 0, c.off, s));
-  char *b = (char *)L->sell_mem;
-  L->sg_col = (int16_t *)(b + o_gc);
-  L->sg_val = (__nv_bfloat16 *)(b + o_gv);
-  L->st_col = (int16_t *)(b + o_tc);
-  L->st_val = (__nv_bfloat16 *)(b + o_tv);
-  k_sell_fill<<<grid_stream(h, N), kThreads, 0, s>>>(N, L->gptr, L->gcol, L->sg_ptr,
-                                                     L->sg_col, L->g2sg);
-  k_sell_fill<<<grid_stream(h, N), kThreads, 0, s>>>(N, L->tptr, L->tcol, L->st_ptr,
-                                                     L->st_col, L->t2st);
-  CUDA_TRY(cudaGetLastError());
+  size_t o_wd = take_n<int>(c, nsl);
+  size_t o_vc = take_n<int>(c, nsl), o_oc = take_n<int>(c, nsl);
+  size_t o_un = take_n<int>(c, nsl), o_vb = take_n<int>(c, nsl + 1);
+  size_t o_ob = take_n<int>(c, nsl + 1);
+  size_t o_sm = take_n<int>(c, nsl / kScanBlock + 1);
+  size_t o_tot = take_n<unsigned long long>(c, 4);
+  void *tmp = nullptr;
+  CUDA_TRY(cudaMalloc(&tmp, c.off));
+  char *t = (char *)tmp;
+  int *wd = (int *)(t + o_wd);
+  int *vc = (int *)(t + o_vc), *oc = (int *)(t + o_oc), *un = (int *)(t + o_un);
+  int *vb = (int *)(t + o_vb), *ob = (int *)(t + o_ob), *sm = (int *)(t + o_sm);
+  unsigned long long *tot = (unsigned long long *)(t + o_tot);
+  auto fail_free = [&](cudaError_t e) {
+    cudaFree(tmp);
+    return fail(CGX_ERROR_CUDA, cudaGetErrorString(e));
+  };
+  cudaError_t e = cudaMemsetAsync(tot, 0, 4 * sizeof(unsigned long long), s);
+  if (e != cudaSuccess) return fail_free(e);
+  const int wgrid = grid_stream(h, (size_t)nsl * 32);
+  k_sellu_plan<<<wgrid, kThreads, 0, s>>>(N, ptr, col, wd, vc, oc, un, tot);
+  unsigned long long ht[4] = {0, 0, 0, 0};
+  if ((e = cudaGetLastError()) != cudaSuccess ||
+      (e = cudaMemcpyAsync(ht, tot, sizeof(ht), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+      (e = cudaStreamSynchronize(s)) != cudaSuccess)
+    return fail_free(e);
+  // Value slots: 128 per group.
+  if (128 * ht[0] + 128 >= (unsigned long long)INT_MAX || ht[1] >= (unsigned long long)INT_MAX) {
+    cudaFree(tmp);
+    return CGX_SUCCESS;
+  }
+  Carver d;
+  size_t o_meta = take_n<int4>(d, nsl), o_off = take_n<int>(d, ht[1]);
+  size_t o_map = take_n<int>(d, nnz);
+  if ((e = scan(h, nsl, vc, vb, sm)) != cudaSuccess ||
+      (e = scan(h, nsl, oc, ob, sm)) != cudaSuccess ||
+      (e = cudaMalloc(&S.mem, d.off)) != cudaSuccess ||
+      (e = cudaMemsetAsync(S.mem, 0, d.off, s)) != cudaSuccess)
+    return fail_free(e);
+  char *b = (char *)S.mem;
+  S.meta = (int4 *)(b + o_meta);
+  S.off = (int *)(b + o_off);
+  S.map = (int *)(b + o_map);
+  k_sellu_fill<<<wgrid, kThreads, 0, s>>>(N, ptr, col, vb, ob, wd, un, S.meta,
+                                          S.off, S.map);
+  if ((e = cudaGetLastError()) != cudaSuccess ||
+      (e = cudaStreamSynchronize(s)) != cudaSuccess)
+    return fail_free(e);
+  cudaFree(tmp);
+  S.max_width = (int)ht[3];
+  S.slots = 128 * (size_t)ht[0];
+  S.uniform = (long long)ht[2];
+  S.ok = true;
+  return CGX_SUCCESS;
+}
+
+// SELL-U layouts of G and G^T with their BF16 value arrays (zero padding;
+// k_assemble writes the values through the maps).
+cgx_status build_sell(cgx_handle *h) {
+  Learned *L = h->L;
+  L->sell_ok = false;
+  CGX_TRY(build_sellu(h, L->gptr, L->gcol, (size_t)L->nnzL, L->sg));
+  CGX_TRY(build_sellu(h, L->tptr, L->tcol, (size_t)L->nnzL, L->st));
+  if (!L->sg.ok || !L->st.ok) return CGX_SUCCESS;
+  Carver c;
+  size_t o_g = take_n<__nv_bfloat16>(c, L->sg.slots);
+  size_t o_t = take_n<__nv_bfloat16>(c, L->st.slots);
+  if (L->sell_val) cudaFree(L->sell_val);
+  L->sell_val = nullptr;
+  CUDA_TRY(cudaMalloc(&L->sell_val, c.off));
+  CUDA_TRY(cudaMemsetAsync(L->sell_val, 0, c.off, h->stream));
+  L->sg_val = (__nv_bfloat16 *)((char *)L->sell_val + o_g);
+  L->st_val = (__nv_bfloat16 *)((char *)L->sell_val + o_t);
   L->sell_ok = true;
   return CGX_SUCCESS;
 }
@@ -1659,7 +1765,7 @@ cudaError_t gnn_forward(cgx_handle *h, const float *P, bool scaled) {
       L->nnzL, L->grow, L->gcol, L->g2a, L->ahat, L->o, L->ghat, L->dis,
       L->g2t, scaled ? L->gs : nullptr, scaled ? L->gts : nullptr,
       scaled && L->sell_ok ? L->sg_val : nullptr,
-      scaled && L->sell_ok ? L->st_val : nullptr, L->g2sg, L->t2st);
+      scaled && L->sell_ok ? L->st_val : nullptr, L->sg.map, L->st.map);
   return cudaGetLastError();
 }
 

@@ -246,76 +246,6 @@ __global__ void __launch_bounds__(kThreads)
   op.finish(acc, st, partials);
 }
 
-// ---------------------------------------------------------------------------
-// Sliced ELL (SELL-32) SpMV for short rows (the learned factor G and G^T, ~4
-// entries per row on a 7-point matrix). Rows are taken in order in slices of
-// 32; slice s holds width(s) = max row length of its rows, stored column-major
-// from sptr[s]: entry k of row s*32 + r at sptr[s] + 32 k + r. Values are
-// BF16, columns 16-bit offsets from the row; padding slots hold value 0 and
-// offset 0. A warp owns a slice (lane = row), so every value/offset load is
-// one coalesced 64-byte access, no row pointers are read, and four gathers
-// per lane are in flight.
-struct SellView {
-  const int *sptr;  // nslices + 1 element offsets
-  const int16_t *col;
-  const __nv_bfloat16 *val;
-  int N;
-};
-
-template <typename Op>
-__global__ void __launch_bounds__(kThreads)
-    k_sell(SellView A, const float *__restrict__ x, Op op, CgState *st,
-           double *partials) {
-  if (op.skip(st)) return;
-  typename Op::Acc acc;
-  constexpr int SPW = 2;  // slices a warp works on at once
-  const int lane = threadIdx.x & 31;
-  const int nslices = (A.N + 31) >> 5;
-  const int warp = (blockIdx.x * kThreads + threadIdx.x) >> 5;
-  const int nwarps = (gridDim.x * kThreads) >> 5;
-  for (int s0 = warp * SPW; s0 < nslices; s0 += nwarps * SPW) {
-    int b[SPW], w[SPW];
-#pragma unroll
-    for (int q = 0; q < SPW; q++) {
-      const int s = min(s0 + q, nslices - 1);
-      b[q] = __ldg(&A.sptr[s]);
-      w[q] = s0 + q < nslices ? (__ldg(&A.sptr[s + 1]) - b[q]) >> 5 : 0;
-    }
-    int wmax = 0;
-#pragma unroll
-    for (int q = 0; q < SPW; q++) wmax = max(wmax, w[q]);
-    float sum[SPW];
-#pragma unroll
-    for (int q = 0; q < SPW; q++) sum[q] = 0.f;
-    for (int k = 0; k < wmax; k += 4) {
-      float xv[SPW][4], vv[SPW][4];
-#pragma unroll
-      for (int q = 0; q < SPW; q++) {
-        const int rr = min(((s0 + q) << 5) + lane, A.N - 1);  // padding lanes: row N-1
-#pragma unroll
-        for (int u = 0; u < 4; u++) {
-          if (k + u < w[q]) {
-            const int slot = b[q] + ((k + u) << 5) + lane;
-            vv[q][u] = __bfloat162float(A.val[slot]);
-            xv[q][u] = __ldg(&x[rr + (int)A.col[slot]]);
-          }
-        }
-      }
-#pragma unroll
-      for (int q = 0; q < SPW; q++)
-#pragma unroll
-        for (int u = 0; u < 4; u++)
-          if (k + u < w[q]) sum[q] = fmaf(vv[q][u], xv[q][u], sum[q]);
-    }
-#pragma unroll
-    for (int q = 0; q < SPW; q++) {
-      const int row = ((s0 + q) << 5) + lane;
-      if (s0 + q < nslices && row < A.N) op.row(row, sum[q], acc);
-    }
-  }
-  op.finish(acc, st, partials);
-}
-
 // Column indices as 16-bit offsets from the row (the compact CRS of the
 // mixed and learned paths); sets *flag if an offset does not fit.
 __global__ void __launch_bounds__(kThreads)
@@ -513,6 +443,14 @@ struct OpInnerQ {
   __device__ void row(int i, float s, Acc &a) const {
     q[i] = s;
     a.a0 = fma((double)__ldg(&p[i]), (double)s, a.a0);
+  }
+  struct Pre {
+    float p;
+  };
+  __device__ Pre prefetch(int i) const { return Pre{__ldg(&p[i])}; }
+  __device__ void row(int i, float s, Acc &a, const Pre &pr) const {
+    q[i] = s;
+    a.a0 = fma((double)pr.p, (double)s, a.a0);
   }
   __device__ void finish(Acc &a, CgState *st, double *partials) const {
     double in[1] = {a.a0}, out[1];
@@ -868,9 +806,12 @@ __global__ void __launch_bounds__(kThreads)
 // y = M r for the first factor of the apply; skipped once the loop stopped.
 struct OpInnerStore {
   using Acc = NoAcc;
+  struct Pre {};
   float *y;
   __device__ bool skip(const CgState *st) const { return st->in_stop != 0; }
   __device__ void row(int i, float s, Acc &) const { y[i] = s; }
+  __device__ Pre prefetch(int) const { return Pre{}; }
+  __device__ void row(int i, float s, Acc &, const Pre &) const { y[i] = s; }
   __device__ void finish(Acc &, CgState *, double *) const {}
 };
 
@@ -885,11 +826,17 @@ struct OpLearnedZ {
   unsigned *ticket;
   __device__ bool skip(const CgState *st) const { return st->in_stop != 0; }
   __device__ void row(int i, float s, Acc &a) const {
-    const float ri = __ldg(&r[i]);
-    const float zi = fmaf(eps * __ldg(&C[i]), ri, s);
+    row(i, s, a, prefetch(i));
+  }
+  struct Pre {
+    float r, c;
+  };
+  __device__ Pre prefetch(int i) const { return Pre{__ldg(&r[i]), __ldg(&C[i])}; }
+  __device__ void row(int i, float s, Acc &a, const Pre &pr) const {
+    const float zi = fmaf(eps * pr.c, pr.r, s);
     z[i] = zi;
     if (start) p[i] = zi;
-    a.a0 = fma((double)ri, (double)zi, a.a0);
+    a.a0 = fma((double)pr.r, (double)zi, a.a0);
   }
   __device__ void finish(Acc &a, CgState *st, double *partials) const {
     double in[1] = {a.a0}, out[1];

@@ -423,7 +423,7 @@ __global__ void k_assemble(int nnzL, const int *__restrict__ grow,
       const float sv = (float)(dis[i] * (double)v);
       gs[e] = sv;
       gts[g2t[e]] = sv;
-      if (sgv) {
+      if (sgv) {  // the SELL-U copies of G and G^T
         const __nv_bfloat16 bv = __float2bfloat16_rn(sv);
         sgv[g2sg[e]] = bv;
         stv[t2st[g2t[e]]] = bv;
@@ -758,36 +758,6 @@ __global__ void k_adam(int n, float *__restrict__ p, float *__restrict__ m,
     m[k] = mk;
     v[k] = vk;
     p[k] -= lr * (mk / c1) / (sqrtf(vk / c2) + eps);
-  }
-}
-
-// SELL-32 build from a CRS pattern: slot count 32 * (max row length) per
-// slice (written to cnt[s] for the scan that gives the slice offsets).
-__global__ void k_sell_count(int N, const int *__restrict__ rp, int *cnt) {
-  const int nslices = (N + 31) >> 5;
-  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nslices;
-       s += gridDim.x * blockDim.x) {
-    int w = 0;
-    for (int r = s * 32; r < min(N, s * 32 + 32); r++)
-      w = max(w, rp[r + 1] - rp[r]);
-    cnt[s] = 32 * w;
-  }
-}
-
-// SELL-32 slot of every CRS entry (map) and its 16-bit column offset; the
-// padding slots keep the zero value / zero offset they were cleared to.
-__global__ void k_sell_fill(int N, const int *__restrict__ rp,
-                            const int *__restrict__ col,
-                            const int *__restrict__ sptr,
-                            int16_t *__restrict__ scol, int *__restrict__ map) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N;
-       i += gridDim.x * blockDim.x) {
-    const int base = sptr[i >> 5] + (i & 31);
-    for (int k = 0; k < rp[i + 1] - rp[i]; k++) {
-      const int e = rp[i] + k, dst = base + (k << 5);
-      scol[dst] = (int16_t)(col[e] - i);
-      map[e] = dst;
-    }
   }
 }
 

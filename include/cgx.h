@@ -219,6 +219,15 @@ cgx_status cgx_gnn_train_step(cgx_gnn *g, cgx_handle *h,
 /* FP64 ||k - A x|| / ||k|| of the current X. */
 cgx_status cgx_true_residual(cgx_handle *h, double *rel);
 
+/* Layout of A's FP32 copy used by the inner SpMV of the mixed and learned
+ * paths (built by the first mixed solve; no counterpart in the reference):
+ * rows in slices of 32, *slices in all, *uniform_slices of them storing one
+ * column offset per slot for all 32 rows (no per-entry index), *value_slots
+ * FP32 values including zero padding. *value_slots = 0: the inner SpMV uses
+ * FP32 CRS (not built yet, or the layout's indices would not fit in int). */
+cgx_status cgx_inner_layout(cgx_handle *h, long long *value_slots,
+                            long long *uniform_slices, long long *slices);
+
 /* MatrixMarket I/O (MatrixCOO::MatrixCOO, Matrix.cpp:13-111). Reads a
  * `matrix coordinate real general|symmetric` file into newly malloc'ed
  * arrays (free them with cgx_free) with the reference's entry order:

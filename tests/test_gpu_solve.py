@@ -146,3 +146,49 @@ def test_mixed_loops_agree(handle):
         assert r["converged"] == 1
     assert out[0][0] == out[1][0] == out[2][0]
     assert np.array_equal(out[0][1], out[1][1]) and np.array_equal(out[0][1], out[2][1])
+
+
+def _shuffle_rows(A, seed):
+    """The same matrix with every row's entries in a random order."""
+    rng = np.random.default_rng(seed)
+    index, value = A.index.copy(), A.value.copy()
+    for i in range(A.N):
+        a, b = A.ptr[i], A.ptr[i + 1]
+        p = a + rng.permutation(b - a)
+        index[a:b], value[a:b] = A.index[p], A.value[p]
+    return G.Crs(A.N, A.ptr, index, value)
+
+
+@pytest.mark.parametrize("case", ["ragged", "unsorted", "wide", "stencil27_odd"])
+def test_mixed_on_irregular_patterns(handle, case):
+    """The FP32 inner SpMV's sliced layout: uniform slices (stencils, with
+    zero-filled missing neighbours at the boundary), per-row slices (ragged
+    random rows, rows whose offsets span more than 32 slots, unsorted rows)
+    and a last slice shorter than 32 rows (N not a multiple of 32)."""
+    if case == "ragged":
+        A = random_crs(1007, max_len=12, seed=3, spd=True)
+    elif case == "unsorted":
+        A = _shuffle_rows(G.diffusion3d(13, stencil=7, seed=4), seed=5)
+    elif case == "wide":
+        A = random_crs(777, max_len=80, seed=4, spd=True)
+    else:
+        A = G.diffusion3d(11, stencil=27, seed=6)
+    b, _ = G.rhs_for(A, seed=7)
+    handle.upload_crs(A.ptr, A.index, A.value)
+    Cd = 1.0 / A.diagonal()
+    handle.upload_jacobi(Cd)
+    handle.set_vector("K", b)
+    handle.fill_vector("X", 0.0)
+    res = handle.solve(max_iterations=20000, tolerance=1e-9, precision=cg.PRECISION_MIXED)
+    x = handle.get_vector("X")
+    assert res["converged"] == 1
+    tr = np.linalg.norm(b - A.matvec(x)) / np.linalg.norm(b)
+    assert tr <= 1e-9
+    _, it_o, outer_o, _ = O.mixed_ir_solve(A.ptr, A.index, A.value, Cd, b)
+    assert abs(res["iterations"] - it_o) <= 0.05 * it_o + 2
+    slots, uniform, slices = handle.inner_layout()
+    assert slices == (A.N + 31) // 32 and slots >= A.nz
+    if case == "stencil27_odd":
+        assert uniform == slices
+    elif case == "unsorted":
+        assert uniform == 0
