@@ -52,17 +52,23 @@ __device__ __forceinline__ float to_float(__nv_bfloat16 v) {
   return __bfloat162float(v);
 }
 
-// Four consecutive slots of one lane (16 bytes of FP32, 8 of BF16).
+// Four consecutive slots of one lane (16 bytes of FP32, 8 of BF16). The
+// values are read once per product, so they bypass L1 (no_allocate) and
+// leave it to the gathers of x, whose windows neighbouring slices share.
 __device__ __forceinline__ float4 load_group(const float *p) {
-  return __ldg(reinterpret_cast<const float4 *>(p));
+  float4 v;
+  asm("ld.global.nc.L1::no_allocate.v4.f32 {%0,%1,%2,%3}, [%4];"
+      : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+      : "l"(p));
+  return v;
 }
 __device__ __forceinline__ float4 load_group(const __nv_bfloat16 *p) {
-  const uint2 u = __ldg(reinterpret_cast<const uint2 *>(p));
+  uint2 u;
+  asm("ld.global.nc.L1::no_allocate.v2.u32 {%0,%1}, [%2];"
+      : "=r"(u.x), "=r"(u.y)
+      : "l"(p));
   return make_float4(__uint_as_float(u.x << 16), __uint_as_float(u.x & 0xffff0000u),
                      __uint_as_float(u.y << 16), __uint_as_float(u.y & 0xffff0000u));
-}
-__device__ __forceinline__ float comp(const float4 &v, int c) {
-  return c == 0 ? v.x : c == 1 ? v.y : c == 2 ? v.z : v.w;
 }
 
 // SELL-U SpMV with the row epilogue of Op (the same Ops as k_crs, with the
@@ -122,30 +128,43 @@ __global__ void __launch_bounds__(kThreads)
 #pragma unroll
     for (int q = 0; q < SPW; q++) sum[q] = 0.f;
     if (fast) {
-      int ol[SPW];
+      // Slots past a slice's width: inside its last group they hold value 0
+      // and offset 0 (lanes >= w of ol load 0); whole groups past it re-read
+      // the last group and are zeroed. Gathers are clamped to [0, N) with one
+      // unsigned min (a negative column wraps to a large value).
+      int ol[SPW], ng[SPW];
 #pragma unroll
-      for (int q = 0; q < SPW; q++)
+      for (int q = 0; q < SPW; q++) {
         ol[q] = lane < w[q] ? __ldg(&A.off[ob[q] + lane]) : 0;
+        ng[q] = (w[q] + 3) >> 2;
+      }
+      const unsigned nmax = (unsigned)(A.N - 1);
       for (int k0 = 0; k0 < wmax; k0 += U) {
         float4 a[SPW][NG];
         float b[SPW][U];
 #pragma unroll
         for (int q = 0; q < SPW; q++) {
-          const int gl = max(((w[q] + 3) >> 2) - 1, 0), wl = max(w[q] - 1, 0);
 #pragma unroll
-          for (int g = 0; g < NG; g++)
-            a[q][g] = load_group(A.val + ((((vb[q] + min((k0 >> 2) + g, gl)) << 5) + lane) << 2));
+          for (int g = 0; g < NG; g++) {
+            const int gi = (k0 >> 2) + g;
+            a[q][g] = load_group(A.val + ((((vb[q] + min(gi, max(ng[q] - 1, 0))) << 5) + lane) << 2));
+          }
 #pragma unroll
           for (int u = 0; u < U; u++) {
-            const int o = __shfl_sync(0xffffffffu, ol[q], min(k0 + u, wl) & 31);
-            b[q][u] = __ldg(&x[min(max(row[q] + o, 0), A.N - 1)]);
+            const int o = __shfl_sync(0xffffffffu, ol[q], (k0 + u) & 31);
+            b[q][u] = __ldg(&x[min((unsigned)(row[q] + o), nmax)]);
           }
         }
 #pragma unroll
         for (int q = 0; q < SPW; q++)
 #pragma unroll
-          for (int u = 0; u < U; u++)
-            sum[q] = fmaf(k0 + u < w[q] ? comp(a[q][u >> 2], u & 3) : 0.f, b[q][u], sum[q]);
+          for (int g = 0; g < NG; g++) {
+            const float4 v = (k0 >> 2) + g < ng[q] ? a[q][g] : make_float4(0.f, 0.f, 0.f, 0.f);
+            sum[q] = fmaf(v.x, b[q][4 * g + 0], sum[q]);
+            sum[q] = fmaf(v.y, b[q][4 * g + 1], sum[q]);
+            sum[q] = fmaf(v.z, b[q][4 * g + 2], sum[q]);
+            sum[q] = fmaf(v.w, b[q][4 * g + 3], sum[q]);
+          }
       }
     } else {
 #pragma unroll
