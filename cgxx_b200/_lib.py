@@ -112,6 +112,7 @@ PROTOTYPES = {
     "cgx_host_free": [_P],
     "cgx_dot_noalloc": [_P, _P, _I, _P, _P],
     "cgx_gnn_param_count": [],
+    "cgx_gnn_set_probes": [_P, _I, _I, C.c_float],
     "cgx_gnn_create": [C.POINTER(_P), _I, _P],
     "cgx_gnn_destroy": [_P],
     "cgx_gnn_set_params": [_P, _P],
@@ -366,6 +367,13 @@ class Gnn:
         check(self._lib.cgx_gnn_loss_grad(self._g, handle._h, pp, seed, C.byref(loss),
                                           grad.ctypes.data_as(C.c_void_p)))
         return loss.value, grad
+
+    def set_probes(self, smooth_steps=0, smooth_cols=0, smooth_scale=1.0):
+        """Probe recipe of loss_grad (probes=None) and train_step: the last
+        smooth_cols Rademacher columns take smooth_steps damped-Jacobi steps
+        on Ahat and are scaled by smooth_scale."""
+        check(self._lib.cgx_gnn_set_probes(self._g, int(smooth_steps), int(smooth_cols),
+                                           float(smooth_scale)))
 
     def train_step(self, handle, seed, lr):
         loss = C.c_float()

@@ -228,6 +228,9 @@ struct cgx_gnn {
   int device = 0;
   float *params = nullptr, *m = nullptr, *v = nullptr;
   int step = 0;
+  // Probe recipe (cgx_gnn_set_probes).
+  int smooth_steps = 0, smooth_cols = 0;
+  float smooth_scale = 1.f;
 };
 
 static void drop_graphs(cgx_handle *h) {
@@ -2061,6 +2064,37 @@ cgx_status cgx_learned_get_factor(cgx_handle *h, int *nnzL, float *ghat,
   return CGX_SUCCESS;
 }
 
+// Rademacher probes from `seed` into L->V, then the network's smoothing of
+// its last columns.
+static cudaError_t make_probes(const cgx_gnn *gn, cgx_handle *h,
+                               unsigned long long seed) {
+  Learned *L = h->L;
+  cudaStream_t s = h->stream;
+  const int gs = grid_stream(h, (size_t)h->N * S);
+  k_rademacher<<<gs, kThreads, 0, s>>>(h->N, seed, L->V);
+  for (int k = 0; k < gn->smooth_steps && gn->smooth_cols > 0; k++) {
+    k_spmm8<<<grid_stream(h, h->N), kThreads, 0, s>>>(h->N, h->ptr, h->index,
+                                                       L->ahat, nullptr, L->V, L->T1);
+    k_smooth_probes<<<gs, kThreads, 0, s>>>(
+        h->N, L->V, L->T1, 2.f / 3.f,
+        k == gn->smooth_steps - 1 ? gn->smooth_scale : 1.f, gn->smooth_cols);
+  }
+  return cudaGetLastError();
+}
+
+cgx_status cgx_gnn_set_probes(cgx_gnn *gn, int smooth_steps, int smooth_cols,
+                              float smooth_scale) {
+  if (!gn) return fail(CGX_ERROR_INVALID_ARGUMENT, "network is NULL");
+  if (smooth_steps < 0 || smooth_cols < 0 || smooth_cols > S ||
+      !(smooth_scale > 0.f))
+    return fail(CGX_ERROR_INVALID_ARGUMENT,
+                "need smooth_steps >= 0, 0 <= smooth_cols <= 8, smooth_scale > 0");
+  gn->smooth_steps = smooth_steps;
+  gn->smooth_cols = smooth_cols;
+  gn->smooth_scale = smooth_scale;
+  return CGX_SUCCESS;
+}
+
 cgx_status cgx_gnn_loss_grad(cgx_gnn *gn, cgx_handle *h, const float *probes,
                              unsigned long long seed, float *loss, float *grad) {
   CGX_TRY(need_matrix(h));
@@ -2074,7 +2108,7 @@ cgx_status cgx_gnn_loss_grad(cgx_gnn *gn, cgx_handle *h, const float *probes,
     CUDA_TRY(cudaMemcpyAsync(L->V, probes, sizeof(float) * h->N * S,
                              cudaMemcpyHostToDevice, s));
   else
-    k_rademacher<<<grid_stream(h, (size_t)h->N * S), kThreads, 0, s>>>(h->N, seed, L->V);
+    CUDA_TRY(make_probes(gn, h, seed));
   CUDA_TRY(gnn_forward(h, gn->params, false));
   CUDA_TRY(gnn_backward(h, gn->params));
   if (loss)
@@ -2097,7 +2131,7 @@ cgx_status cgx_gnn_train_step(cgx_gnn *gn, cgx_handle *h, unsigned long long see
   CGX_TRY(learned_train_alloc(h));
   Learned *L = h->L;
   cudaStream_t s = h->stream;
-  k_rademacher<<<grid_stream(h, (size_t)h->N * S), kThreads, 0, s>>>(h->N, seed, L->V);
+  CUDA_TRY(make_probes(gn, h, seed));
   CUDA_TRY(gnn_forward(h, gn->params, false));
   CUDA_TRY(gnn_backward(h, gn->params));
   gn->step++;

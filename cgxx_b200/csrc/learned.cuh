@@ -761,6 +761,18 @@ __global__ void k_adam(int n, float *__restrict__ p, float *__restrict__ m,
   }
 }
 
+// Smoothed probe columns: for the last `cols` of the S columns, V <- sc (V -
+// om T) with T = Ahat V (one damped-Jacobi step on the Jacobi-scaled matrix;
+// sc is the column scale, applied once after the last step).
+__global__ void k_smooth_probes(int N, float *__restrict__ V,
+                                const float *__restrict__ T, float om, float sc,
+                                int cols) {
+  const size_t n = (size_t)N * S;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    if ((int)(i % S) >= S - cols) V[i] = sc * fmaf(-om, T[i], V[i]);
+}
+
 // Rademacher probes from a counter-based hash: V[i*S+s] = +-1.
 __global__ void k_rademacher(int N, unsigned long long seed, float *V) {
   const int total = N * S;

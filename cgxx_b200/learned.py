@@ -8,9 +8,18 @@ cgx_learned_*); this module orchestrates them through the C ABI:
       (7-point diffusion, coefficient exp(g), g a Gaussian random field with
       sigma ~ U[0.5, 2] and correlation length ~ U[4, 16] cells), Adam on
       the Hutchinson loss ||(Ghat^T Ahat Ghat - I) V||^2 with Rademacher
-      probes V, then PCG on the held-out fields: learned G G^T against
-      Jacobi, both FP32-inner / FP64-refinement to a 1e-9 FP64 true
+      probes V (by default half of the 8 columns smoothed by 3 damped-Jacobi
+      steps and scaled by 3, which weights the smooth end of the spectrum
+      that limits CG), then PCG on the held-out fields: learned G G^T
+      against Jacobi, both FP32-inner / FP64-refinement to a 1e-9 FP64 true
       residual, and plain FP64 Jacobi-CG.
+
+      Checkpoint selection: the untrained network and the network after
+      each epoch are scored by the median learned-PCG iteration count on 16
+      held-out fields; the best is written (the untrained network when no
+      epoch improves on it). On this family the untrained network already
+      reproduces the quality of a factorized sparse approximate inverse on
+      the pattern of tril(A), so training has little room to gain.
 
 Weight file: 8-byte magic b"CGXGNN01", uint32 header length, UTF-8 JSON
 header (parameter count, dtype, layout, seed, training configuration and its
@@ -121,6 +130,11 @@ def main(argv=None):
     t.add_argument("--epochs", type=int, default=4)
     t.add_argument("--lr", type=float, default=2e-3)
     t.add_argument("--eps", type=float, default=1e-4)
+    t.add_argument("--smooth-steps", type=int, default=3)
+    t.add_argument("--smooth-cols", type=int, default=4)
+    t.add_argument("--smooth-scale", type=float, default=3.0)
+    t.add_argument("--select", type=int, default=16,
+                   help="held-out fields scored for checkpoint selection")
     t.add_argument("--seed", type=int, default=0)
     t.add_argument("--workers", type=int, default=min(16, os.cpu_count() or 1))
     t.add_argument("--out", default=DEFAULT_WEIGHTS)
@@ -175,11 +189,31 @@ def run_training(a):
     else:
         params = init_params(a.seed)
     net = cg.Gnn(0, params)
+    net.set_probes(a.smooth_steps, a.smooth_cols, a.smooth_scale)
+
+    def selection_score(gnn):
+        its = []
+        for k, v in enumerate(ho_vals[:a.select]):
+            h.update_crs_values(v)
+            h.upload_jacobi(_diag_inv(fam, v))
+            b, _ = G.rhs_for(G.Crs(fam.N, fam.ptr, fam.index, v), seed=k)
+            h.set_vector("K", b)
+            h.learned_setup()
+            h.learned_factor(gnn, a.eps)
+            h.fill_vector("X", 0.0)
+            r = h.solve(max_iterations=20000, tolerance=1e-9,
+                        preconditioner=cg.PRECOND_LEARNED, precision=cg.PRECISION_MIXED)
+            its.append(r["iterations"] if r["converged"] else 10 ** 9)
+        return float(np.median(its))
 
     log = []
     t1 = time.time()
     steps = 0
+    selected = 0
     if not a.eval_only:
+        best = (selection_score(net), 0, net.get_params())
+        log.append({"epoch": -1, "selection_median_iterations": best[0]})
+        print(json.dumps(log[-1]), flush=True)
         rng = np.random.default_rng(a.seed)
         for ep in range(a.epochs):
             order = rng.permutation(len(tr_dev))
@@ -190,9 +224,15 @@ def run_training(a):
                 h.learned_setup()
                 losses.append(net.train_step(h, seed=int(rng.integers(1 << 62)), lr=lr))
                 steps += 1
-            log.append({"epoch": ep, "lr": lr, "mean_loss": float(np.mean(losses))})
+            score = selection_score(net)
+            log.append({"epoch": ep, "lr": lr, "mean_loss": float(np.mean(losses)),
+                        "selection_median_iterations": score})
             print(json.dumps(log[-1]), flush=True)
+            if score < best[0]:
+                best = (score, ep + 1, net.get_params())
         torch.cuda.synchronize()
+        selected = best[1]
+        net.set_params(best[2])
     train_s = time.time() - t1
     params = net.get_params()
 
@@ -204,20 +244,22 @@ def run_training(a):
         h.upload_jacobi(_diag_inv(fam, v))
         b, _ = G.rhs_for(G.Crs(fam.N, fam.ptr, fam.index, v), seed=k)
         r = solve_pair(h, fam.ptr, fam.index, v, b, True, net, a.eps)
-        if k < 8:
-            h.learned_setup()
-            h.learned_factor(init_net, a.eps)
-            h.fill_vector("X", 0.0)
-            ri = h.solve(max_iterations=20000, tolerance=1e-9,
-                         preconditioner=cg.PRECOND_LEARNED, precision=cg.PRECISION_MIXED)
-            r["untrained_learned_mixed"] = {"ms": ri["solve_ms"], "iterations": ri["iterations"]}
+        h.learned_setup()
+        h.learned_factor(init_net, a.eps)
+        h.fill_vector("X", 0.0)
+        ri = h.solve(max_iterations=20000, tolerance=1e-9,
+                     preconditioner=cg.PRECOND_LEARNED, precision=cg.PRECISION_MIXED)
+        r["untrained_learned_mixed"] = {"ms": ri["solve_ms"], "iterations": ri["iterations"]}
         res.append(r)
     summary = summarize(res)
     meta = {"seed": a.seed, "steps": steps, "train_seconds": train_s,
+            "selected_epoch": selected,
             "generate_seconds": gen_s,
             "config": {"grid": a.n, "stencil": 7, "train": a.train, "heldout": a.heldout,
                        "sigma": [0.5, 2.0], "corr_len": [4.0, 16.0], "epochs": a.epochs,
                        "lr": a.lr, "eps": a.eps, "probes": 8,
+                       "smooth_steps": a.smooth_steps, "smooth_cols": a.smooth_cols,
+                       "smooth_scale": a.smooth_scale, "select": a.select,
                        "loss": "||(Ghat^T Ahat Ghat - I) V||^2 / (N S), Rademacher V"},
             "log": log, "heldout": summary}
     if not a.eval_only:

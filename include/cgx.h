@@ -205,14 +205,23 @@ cgx_status cgx_learned_factor(cgx_handle *h, cgx_gnn *g, double eps);
  * each optional). */
 cgx_status cgx_learned_get_factor(cgx_handle *h, int *nnzL, float *ghat,
                                   int *rows, int *cols);
+/* Probe recipe of the network's training (no counterpart in the reference):
+ * Rademacher columns from a seed; then the last `smooth_cols` of the 8
+ * columns take `smooth_steps` damped-Jacobi steps V <- V - (2/3) Ahat V on
+ * the Jacobi-scaled matrix and are multiplied by `smooth_scale`, which
+ * weights the loss toward the smooth end of the spectrum. Default 0, 0, 1
+ * (plain Rademacher probes). */
+cgx_status cgx_gnn_set_probes(cgx_gnn *g, int smooth_steps, int smooth_cols,
+                              float smooth_scale);
 /* Hutchinson loss ||(Ghat^T Ahat Ghat - I) V||_F^2 / (N S) for S = 8 probe
- * columns (probes: N*8 floats, node-major, or NULL for Rademacher probes
- * from `seed`) and its gradient w.r.t. the parameters (grad may be NULL). */
+ * columns (probes: N*8 floats, node-major, or NULL for the network's probe
+ * recipe from `seed`) and its gradient w.r.t. the parameters (grad may be
+ * NULL). */
 cgx_status cgx_gnn_loss_grad(cgx_gnn *g, cgx_handle *h, const float *probes,
                              unsigned long long seed, float *loss,
                              float *grad);
-/* One Adam step on Rademacher probes from `seed`; *loss (optional) is the
- * loss before the step. */
+/* One Adam step on the network's probe recipe from `seed`; *loss
+ * (optional) is the loss before the step. */
 cgx_status cgx_gnn_train_step(cgx_gnn *g, cgx_handle *h,
                               unsigned long long seed, float lr, float *loss);
 

@@ -109,6 +109,35 @@ class Graph:
         return torch.zeros_like(V).index_add_(0, self.r, self.ah[:, None] * V[self.c])
 
 
+def rademacher(N, seed):
+    """Probes V[i, s] = +-1 from the counter-based hash of the device's
+    probe generator (splitmix64 finalizer of seed + golden-ratio * (t + 1),
+    t = i * 8 + s; odd -> +1)."""
+    t = np.arange(N * 8, dtype=np.uint64) + np.uint64(1)
+    with np.errstate(over="ignore"):
+        z = np.uint64(seed) + np.uint64(0x9E3779B97F4A7C15) * t
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        z ^= z >> np.uint64(31)
+    return np.where(z & np.uint64(1), 1.0, -1.0).astype(np.float32).reshape(N, 8)
+
+
+def smooth_probes(g: Graph, V, steps, cols, scale, omega=2.0 / 3.0):
+    """The probe recipe's smoothing: the last `cols` columns take `steps`
+    damped-Jacobi steps V <- V - omega Ahat V and are then multiplied by
+    `scale`."""
+    V = torch.tensor(np.asarray(V, np.float32))
+    if steps <= 0 or cols <= 0:
+        return V.numpy()
+    for k in range(steps):
+        T = g.ahat_mv(V)
+        W = V - omega * T
+        if k == steps - 1:
+            W = scale * W
+        V = torch.cat([V[:, :8 - cols], W[:, 8 - cols:]], 1)
+    return V.numpy()
+
+
 def forward(g: Graph, flat):
     """Returns (gdiag[N], goff[n_lower]) in lower-pattern order (row-major,
     storage order within a row) as float32 tensors with autograd."""

@@ -106,6 +106,29 @@ def test_gradient_is_deterministic():
     net.close()
 
 
+def test_probe_recipe_matches_oracle():
+    """Probes made on the device (Rademacher hash, then smoothed columns)
+    equal the oracle's restatement: the loss and gradient from the device's
+    own probes match those from the oracle's probes passed in explicitly."""
+    A = G.diffusion3d(12, 7, seed=4)
+    h = _setup(A)
+    net = cg.Gnn(0, _params(2))
+    gr = GO.Graph(A.ptr, A.index, A.value)
+    seed = 12345
+    l0, g0 = net.loss_grad(h, seed=seed)
+    l1, g1 = net.loss_grad(h, probes=GO.rademacher(A.N, seed))
+    assert l0 == l1 and np.array_equal(g0, g1)
+    net.set_probes(3, 4, 3.0)
+    l2, g2 = net.loss_grad(h, seed=seed)
+    V = GO.smooth_probes(gr, GO.rademacher(A.N, seed), 3, 4, 3.0)
+    l3, g3 = net.loss_grad(h, probes=V)
+    assert abs(l2 - l3) <= 1e-4 * abs(l3)
+    assert np.linalg.norm(g2 - g3) <= 1e-3 * np.linalg.norm(g3)
+    assert abs(l2 - l0) > 1e-3 * abs(l0)  # the recipe changed the probes
+    h.close()
+    net.close()
+
+
 def test_training_lowers_the_loss():
     fam = G.Diffusion7Family(12)
     rng = np.random.default_rng(0)
