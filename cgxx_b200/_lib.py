@@ -102,6 +102,7 @@ PROTOTYPES = {
     "cgx_apply_jacobi": [_P, _I, _I],
     "cgx_solve": [_P, C.POINTER(Options), C.POINTER(Result)],
     "cgx_true_residual": [_P, _PD],
+    "cgx_time_spmv": [_P, _I, _I, _PD],
     "cgx_inner_layout": [_P, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),
                          C.POINTER(C.c_longlong)],
     "cgx_mtx_read": [C.c_char_p, _PI, _PI, C.POINTER(_PI), C.POINTER(_PI),
@@ -285,6 +286,14 @@ class Handle:
         r = C.c_double()
         check(self._lib.cgx_true_residual(self._h, C.byref(r)))
         return r.value
+
+    def time_spmv(self, precision, reps=20):
+        """Average device time (us) of one launch of the solver's fused
+        SpMV (PRECISION_FP64 or PRECISION_MIXED), timed back to back in a
+        CUDA graph; overwrites Q and the last solve's scalars."""
+        us = C.c_double()
+        check(self._lib.cgx_time_spmv(self._h, int(precision), int(reps), C.byref(us)))
+        return us.value
 
     def inner_layout(self):
         """(value_slots, uniform_slices, slices) of A's FP32 copy for the

@@ -185,6 +185,9 @@ struct cgx_handle {
 
   std::vector<GraphEntry> graphs;
   cudaEvent_t ev[8] = {};
+  // Per-kernel timing mode: 4 events for each of kChunk iterations that are
+  // enqueued before the host waits (created on first use).
+  std::vector<cudaEvent_t> evpool;
 
   // Learned preconditioner (cgx_learned_setup / cgx_learned_factor).
   struct Learned *L = nullptr;
@@ -748,6 +751,7 @@ cgx_status cgx_destroy(cgx_handle *h) {
   free_matrix(h);
   for (auto &ev : h->ev)
     if (ev) cudaEventDestroy(ev);
+  for (auto &ev : h->evpool) cudaEventDestroy(ev);
   if (h->scratch) cudaFree(h->scratch);
   if (h->host_st) cudaFreeHost(h->host_st);
   if (h->host_scalar) cudaFreeHost(h->host_scalar);
@@ -1155,6 +1159,35 @@ static cgx_status device_errors(cgx_handle *h) {
   return CGX_SUCCESS;
 }
 
+// Event pool of the per-kernel timing mode.
+static cgx_status ensure_event_pool(cgx_handle *h) {
+  while ((int)h->evpool.size() < 4 * kChunk) {
+    cudaEvent_t e;
+    CUDA_TRY(cudaEventCreate(&e));
+    h->evpool.push_back(e);
+  }
+  return CGX_SUCCESS;
+}
+
+// Adds the three segments (SpMV | update | direction) of the first `ran`
+// iterations of the last chunk; iterations enqueued after the stop ran no
+// kernel work and are not counted.
+static cudaError_t add_segments(cgx_handle *h, int ran, double &t_spmv,
+                                double &t_upd, double &t_dir) {
+  for (int j = 0; j < std::min(ran, kChunk); j++) {
+    float a = 0, b = 0, c = 0;
+    cudaError_t e;
+    if ((e = cudaEventElapsedTime(&a, h->evpool[4 * j], h->evpool[4 * j + 1])) != cudaSuccess ||
+        (e = cudaEventElapsedTime(&b, h->evpool[4 * j + 1], h->evpool[4 * j + 2])) != cudaSuccess ||
+        (e = cudaEventElapsedTime(&c, h->evpool[4 * j + 2], h->evpool[4 * j + 3])) != cudaSuccess)
+      return e;
+    t_spmv += a;
+    t_upd += b;
+    t_dir += c;
+  }
+  return cudaSuccess;
+}
+
 static cgx_status solve_fp64(cgx_handle *h, const cgx_options &o,
                              cgx_result &res) {
   const bool jacobi = o.preconditioner == CGX_PRECONDITIONER_JACOBI;
@@ -1212,22 +1245,16 @@ static cgx_status solve_fp64(cgx_handle *h, const cgx_options &o,
     CUDA_TRY(launch_pcg_setup(h, jacobi));
     double t_spmv = 0, t_upd = 0, t_dir = 0;
     int it = 0;
-    for (; it < o.max_iterations; it++) {
-      CUDA_TRY(launch_pcg_iteration(h, jacobi, h->ev));
-      CUDA_TRY(cudaMemcpyAsync(h->host_scalar, &h->st->stop, sizeof(int),
-                               cudaMemcpyDeviceToHost, s));
-      CUDA_TRY(cudaStreamSynchronize(s));
-      float a = 0, b = 0, c = 0;
-      CUDA_TRY(cudaEventElapsedTime(&a, h->ev[0], h->ev[1]));
-      CUDA_TRY(cudaEventElapsedTime(&b, h->ev[1], h->ev[2]));
-      CUDA_TRY(cudaEventElapsedTime(&c, h->ev[2], h->ev[3]));
-      t_spmv += a;
-      t_upd += b;
-      t_dir += c;
-      if (*(int *)h->host_scalar) {
-        it++;
-        break;
-      }
+    CGX_TRY(ensure_event_pool(h));
+    const int maxChunks = o.max_iterations / kChunk + 2;
+    for (int c = 0; c < maxChunks; c++) {
+      for (int j = 0; j < kChunk; j++)
+        CUDA_TRY(launch_pcg_iteration(h, jacobi, &h->evpool[4 * j]));
+      CGX_TRY(pull_state(h));
+      const int now = h->host_st->iteration;
+      CUDA_TRY(add_segments(h, now - it, t_spmv, t_upd, t_dir));
+      it = now;
+      if (h->host_st->stop) break;
     }
     CUDA_TRY(cudaEventRecord(h->ev[5], s));
     CGX_TRY(pull_state(h));
@@ -1496,30 +1523,38 @@ static cgx_status solve_mixed(cgx_handle *h, const cgx_options &o,
             ticket(h, kTicketInnerStart));
         CUDA_TRY(cudaGetLastError());
       }
-      const int maxLaunches = o.max_iterations + 2;
-      for (int l = 0; l < maxLaunches; l++) {
-        if (learned) {
-          CUDA_TRY(launch_learned_iteration(
-              h, o.loop == CGX_LOOP_KERNELS ? h->ev : nullptr));
-        } else if (o.loop == CGX_LOOP_CHUNKED) {
-          CUDA_TRY(cudaGraphLaunch(gj->exec, s));
-        } else {
-          CUDA_TRY(launch_inner_iteration(h, h->ev));
+      if (o.loop == CGX_LOOP_KERNELS) {
+        // kChunk iterations per host wait; their kernels skip once the
+        // inner loop stopped.
+        CGX_TRY(ensure_event_pool(h));
+        int counted = h->host_st->total_inner;
+        const int maxChunks = o.max_iterations / kChunk + 2;
+        for (int c = 0; c < maxChunks; c++) {
+          for (int j = 0; j < kChunk; j++) {
+            if (learned)
+              CUDA_TRY(launch_learned_iteration(h, &h->evpool[4 * j]));
+            else
+              CUDA_TRY(launch_inner_iteration(h, &h->evpool[4 * j]));
+          }
+          CGX_TRY(pull_state(h));
+          const int now = h->host_st->total_inner;
+          CUDA_TRY(add_segments(h, now - counted, t_spmv, t_upd, t_dir));
+          launches += now - counted;
+          counted = now;
+          if (h->host_st->in_stop) break;
         }
-        CUDA_TRY(cudaMemcpyAsync(h->host_scalar, &h->st->in_stop, sizeof(int),
-                                 cudaMemcpyDeviceToHost, s));
-        CUDA_TRY(cudaStreamSynchronize(s));
-        if (o.loop == CGX_LOOP_KERNELS) {
-          float a = 0, b = 0, c = 0;
-          CUDA_TRY(cudaEventElapsedTime(&a, h->ev[0], h->ev[1]));
-          CUDA_TRY(cudaEventElapsedTime(&b, h->ev[1], h->ev[2]));
-          CUDA_TRY(cudaEventElapsedTime(&c, h->ev[2], h->ev[3]));
-          t_spmv += a;
-          t_upd += b;
-          t_dir += c;
-          launches++;
+      } else {
+        const int maxLaunches = o.max_iterations + 2;
+        for (int l = 0; l < maxLaunches; l++) {
+          if (learned)
+            CUDA_TRY(launch_learned_iteration(h, nullptr));
+          else
+            CUDA_TRY(cudaGraphLaunch(gj->exec, s));
+          CUDA_TRY(cudaMemcpyAsync(h->host_scalar, &h->st->in_stop, sizeof(int),
+                                   cudaMemcpyDeviceToHost, s));
+          CUDA_TRY(cudaStreamSynchronize(s));
+          if (*(int *)h->host_scalar) break;
         }
-        if (*(int *)h->host_scalar) break;
       }
       CUDA_TRY(outer_update());
     }
@@ -2202,6 +2237,56 @@ cgx_status cgx_solve(cgx_handle *h, const cgx_options *opts,
   if (o.compute_true_residual && o.precision == CGX_PRECISION_FP64)
     CGX_TRY(cgx_true_residual(h, &res.true_residual));
   if (result) *result = res;
+  return CGX_SUCCESS;
+}
+
+cgx_status cgx_time_spmv(cgx_handle *h, cgx_precision precision, int reps,
+                         double *us_per_launch) {
+  CGX_TRY(need_matrix(h));
+  if (reps < 1 || reps > 1000 || !us_per_launch)
+    return fail(CGX_ERROR_INVALID_ARGUMENT, "need 1 <= reps <= 1000 and a result pointer");
+  if (precision != CGX_PRECISION_FP64 && precision != CGX_PRECISION_MIXED)
+    return fail(CGX_ERROR_INVALID_ARGUMENT, "unknown precision");
+  DeviceGuard guard(h->device);
+  if (precision == CGX_PRECISION_MIXED) {
+    if (h->format != CGX_FORMAT_CRS)
+      return fail(CGX_ERROR_UNSUPPORTED, "the FP32 inner SpMV needs CRS");
+    CGX_TRY(ensure_f32(h));
+  }
+  // The products must not skip: clear the stop flags of the last solve.
+  CGX_TRY(pull_state(h));
+  h->host_st->stop = 0;
+  h->host_st->finished = 0;
+  h->host_st->in_stop = 0;
+  h->host_st->in_finished = 0;
+  h->host_st->use_cond = 0;
+  CGX_TRY(push_state(h));
+  cudaStream_t s = h->stream;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  cudaError_t e = cudaSuccess;
+  for (int r = 0; r < reps && e == cudaSuccess; r++)
+    e = precision == CGX_PRECISION_FP64
+            ? launch_spmv(h, h->vec[CGX_VECTOR_P],
+                          OpPcgQ{h->vec[CGX_VECTOR_P], h->vec[CGX_VECTOR_Q],
+                                 ticket(h, kTicketQ)})
+            : launch_inner_q(h);
+  const cudaError_t ec = cudaStreamEndCapture(s, &graph);
+  if (e == cudaSuccess) e = ec;
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+  float ms = 0;
+  if (e == cudaSuccess) e = cudaGraphLaunch(exec, s);  // warm-up
+  if (e == cudaSuccess) e = cudaEventRecord(h->ev[0], s);
+  if (e == cudaSuccess) e = cudaGraphLaunch(exec, s);
+  if (e == cudaSuccess) e = cudaEventRecord(h->ev[1], s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, h->ev[0], h->ev[1]);
+  if (exec) cudaGraphExecDestroy(exec);
+  if (graph) cudaGraphDestroy(graph);
+  CUDA_TRY(e);
+  CGX_TRY(device_errors(h));
+  *us_per_launch = 1000.0 * ms / reps;
   return CGX_SUCCESS;
 }
 

@@ -228,6 +228,16 @@ cgx_status cgx_gnn_train_step(cgx_gnn *g, cgx_handle *h,
 /* FP64 ||k - A x|| / ||k|| of the current X. */
 cgx_status cgx_true_residual(cgx_handle *h, double *rel);
 
+/* Device time of the solver's SpMV alone (no counterpart in the
+ * reference): `reps` back-to-back launches of the fused product the solve
+ * runs (FP64: q = A p with <p,q> on the uploaded format; MIXED: the FP32
+ * inner q = A p with <p,q>) are captured into a CUDA graph and timed with
+ * CUDA events on the handle's stream after one untimed launch of the graph;
+ * *us_per_launch is the average. Uses the current P (FP64) or inner p (MIXED)
+ * and overwrites Q, the inner q and the solver scalars of the last solve. */
+cgx_status cgx_time_spmv(cgx_handle *h, cgx_precision precision, int reps,
+                         double *us_per_launch);
+
 /* Layout of A's FP32 copy used by the inner SpMV of the mixed and learned
  * paths (built by the first mixed solve; no counterpart in the reference):
  * rows in slices of 32, *slices in all, *uniform_slices of them storing one

@@ -192,3 +192,30 @@ def test_mixed_on_irregular_patterns(handle, case):
         assert uniform == slices
     elif case == "unsorted":
         assert uniform == 0
+
+
+def test_time_spmv_measures_the_fused_product(handle):
+    """cgx_time_spmv times the solver's own SpMV (FP64 and the FP32 inner
+    one) back to back, and a solve afterwards is unaffected."""
+    A = G.diffusion3d(24, stencil=7, seed=8)
+    b, _ = G.rhs_for(A, seed=8)
+    handle.upload_crs(A.ptr, A.index, A.value)
+    handle.upload_jacobi(1.0 / A.diagonal())
+    handle.set_vector("K", b)
+    handle.fill_vector("X", 0.0)
+    r1 = handle.solve(max_iterations=5000, tolerance=1e-9)
+    x1 = handle.get_vector("X")
+    handle.fill_vector("X", 0.0)
+    handle.solve(max_iterations=5000, tolerance=1e-9, precision=cg.PRECISION_MIXED)
+    t64 = handle.time_spmv(cg.PRECISION_FP64, reps=5)
+    t32 = handle.time_spmv(cg.PRECISION_MIXED, reps=5)
+    assert 0 < t32 < 1e4 and 0 < t64 < 1e4
+    # q = A p of the last FP64 product, checked against the CPU.
+    p = handle.get_vector("P")
+    assert np.allclose(handle.get_vector("Q"), A.matvec(p), rtol=1e-12, atol=0)
+    handle.fill_vector("X", 0.0)
+    r2 = handle.solve(max_iterations=5000, tolerance=1e-9)
+    assert r2["iterations"] == r1["iterations"]
+    assert np.array_equal(handle.get_vector("X"), x1)
+    with pytest.raises(cg.CgxError):
+        handle.time_spmv(cg.PRECISION_FP64, reps=0)
