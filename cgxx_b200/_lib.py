@@ -113,7 +113,8 @@ PROTOTYPES = {
     "cgx_host_free": [_P],
     "cgx_dot_noalloc": [_P, _P, _I, _P, _P],
     "cgx_gnn_param_count": [],
-    "cgx_gnn_set_probes": [_P, _I, _I, C.c_float],
+    "cgx_gnn_set_probes": [_P, _I, _I, C.c_float, _I],
+    "cgx_learned_capture_residual": [_P, _I],
     "cgx_gnn_create": [C.POINTER(_P), _I, _P],
     "cgx_gnn_destroy": [_P],
     "cgx_gnn_set_params": [_P, _P],
@@ -314,6 +315,11 @@ class Handle:
     def learned_setup(self):
         check(self._lib.cgx_learned_setup(self._h))
 
+    def learned_capture_residual(self, col):
+        """Store r = K - A X (Jacobi-scaled, unit RMS) as probe column col
+        of the learned state (see Gnn.set_probes)."""
+        check(self._lib.cgx_learned_capture_residual(self._h, int(col)))
+
     def learned_factor(self, gnn, eps=0.0):
         check(self._lib.cgx_learned_factor(self._h, gnn._g, float(eps)))
 
@@ -377,12 +383,13 @@ class Gnn:
                                           grad.ctypes.data_as(C.c_void_p)))
         return loss.value, grad
 
-    def set_probes(self, smooth_steps=0, smooth_cols=0, smooth_scale=1.0):
+    def set_probes(self, smooth_steps=0, smooth_cols=0, smooth_scale=1.0, residual_cols=0):
         """Probe recipe of loss_grad (probes=None) and train_step: the last
-        smooth_cols Rademacher columns take smooth_steps damped-Jacobi steps
-        on Ahat and are scaled by smooth_scale."""
+        residual_cols columns are the handle's residual snapshots, the
+        smooth_cols before them Rademacher columns smoothed by smooth_steps
+        damped-Jacobi steps on Ahat and scaled by smooth_scale."""
         check(self._lib.cgx_gnn_set_probes(self._g, int(smooth_steps), int(smooth_cols),
-                                           float(smooth_scale)))
+                                           float(smooth_scale), int(residual_cols)))
 
     def train_step(self, handle, seed, lr):
         loss = C.c_float()

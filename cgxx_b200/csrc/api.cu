@@ -223,6 +223,9 @@ struct Learned {
         *dpre = nullptr;
   float *partial = nullptr, *grad = nullptr, *loss = nullptr;
   float *gtmp = nullptr;  // two reduced [W*W | W] blocks of a layer gradient
+  float *snap = nullptr;  // residual snapshots (probe columns), N x S
+  double *snap_scale = nullptr;
+  unsigned snap_valid = 0;  // bit c: column c holds a snapshot of this matrix
   bool has_factor = false;
   float eps = 0.f;
 };
@@ -232,7 +235,7 @@ struct cgx_gnn {
   float *params = nullptr, *m = nullptr, *v = nullptr;
   int step = 0;
   // Probe recipe (cgx_gnn_set_probes).
-  int smooth_steps = 0, smooth_cols = 0;
+  int smooth_steps = 0, smooth_cols = 0, residual_cols = 0;
   float smooth_scale = 1.f;
 };
 
@@ -1655,7 +1658,7 @@ cgx_status learned_train_alloc(cgx_handle *h) {
   Carver c;
   size_t o[20];
   int k = 0;
-  for (int q = 0; q < 6; q++) o[k++] = take_n<float>(c, (size_t)N * S);
+  for (int q = 0; q < 7; q++) o[k++] = take_n<float>(c, (size_t)N * S);
   o[k++] = take_n<float>(c, L->nnzL);                 // dg
   o[k++] = take_n<float>(c, (size_t)N * NOUT);        // dO
   for (int q = 0; q < 5; q++) o[k++] = take_n<float>(c, (size_t)N * W);
@@ -1663,6 +1666,7 @@ cgx_status learned_train_alloc(cgx_handle *h) {
   o[k++] = take_n<float>(c, NPARAMS);                 // grad
   o[k++] = take_n<float>(c, 4);                       // loss
   o[k++] = take_n<float>(c, 2 * (W * W + W));         // gtmp
+  o[k++] = take_n<double>(c, 1);                      // snap_scale
   size_t o_agg[3], o_pre[4];
   for (int q = 0; q < 3; q++) o_agg[q] = take_n<__nv_bfloat16>(c, (size_t)N * W);
   for (int q = 0; q < 4; q++) o_pre[q] = take_n<float>(c, (size_t)N * W);
@@ -1676,6 +1680,7 @@ cgx_status learned_train_alloc(cgx_handle *h) {
   L->rho = (float *)(b + o[k++]);
   L->dT2 = (float *)(b + o[k++]);
   L->dT1 = (float *)(b + o[k++]);
+  L->snap = (float *)(b + o[k++]);
   L->dg = (float *)(b + o[k++]);
   L->dO = (float *)(b + o[k++]);
   L->dh = (float *)(b + o[k++]);
@@ -1687,6 +1692,7 @@ cgx_status learned_train_alloc(cgx_handle *h) {
   L->grad = (float *)(b + o[k++]);
   L->loss = (float *)(b + o[k++]);
   L->gtmp = (float *)(b + o[k++]);
+  L->snap_scale = (double *)(b + o[k++]);
   for (int q = 0; q < 3; q++) L->agg[q] = (__nv_bfloat16 *)(b + o_agg[q]);
   for (int q = 0; q < 4; q++) L->pre[q] = (float *)(b + o_pre[q]);
   return CGX_SUCCESS;
@@ -1992,6 +1998,7 @@ cgx_status cgx_learned_setup(cgx_handle *h) {
       return fail(CGX_ERROR_UNSUPPORTED,
                   "learned preconditioner: a diagonal entry is missing or not positive");
     L->has_factor = false;
+    L->snap_valid = 0;  // snapshots belong to the previous values
     return CGX_SUCCESS;  // pattern unchanged (cgx_update_crs_values)
   }
   // Lower/upper totals.
@@ -2101,32 +2108,65 @@ cgx_status cgx_learned_get_factor(cgx_handle *h, int *nnzL, float *ghat,
 
 // Rademacher probes from `seed` into L->V, then the network's smoothing of
 // its last columns.
-static cudaError_t make_probes(const cgx_gnn *gn, cgx_handle *h,
-                               unsigned long long seed) {
+// Columns: [0, S - rc - sc) Rademacher, [S - rc - sc, S - rc) smoothed
+// Rademacher, [S - rc, S) the handle's residual snapshots (rc =
+// residual_cols, sc = smooth_cols).
+static cgx_status make_probes(const cgx_gnn *gn, cgx_handle *h,
+                              unsigned long long seed) {
   Learned *L = h->L;
   cudaStream_t s = h->stream;
+  const int rc = gn->residual_cols, c1 = S - rc, c0 = c1 - gn->smooth_cols;
+  const unsigned need = rc > 0 ? (((1u << rc) - 1u) << c1) : 0u;
+  if ((L->snap_valid & need) != need)
+    return fail(CGX_ERROR_INVALID_STATE,
+                "the probe recipe needs residual snapshots of this matrix "
+                "(cgx_learned_capture_residual)");
   const int gs = grid_stream(h, (size_t)h->N * S);
   k_rademacher<<<gs, kThreads, 0, s>>>(h->N, seed, L->V);
-  for (int k = 0; k < gn->smooth_steps && gn->smooth_cols > 0; k++) {
+  for (int k = 0; k < gn->smooth_steps && c1 > c0; k++) {
     k_spmm8<<<grid_stream(h, h->N), kThreads, 0, s>>>(h->N, h->ptr, h->index,
                                                        L->ahat, nullptr, L->V, L->T1);
     k_smooth_probes<<<gs, kThreads, 0, s>>>(
         h->N, L->V, L->T1, 2.f / 3.f,
-        k == gn->smooth_steps - 1 ? gn->smooth_scale : 1.f, gn->smooth_cols);
+        k == gn->smooth_steps - 1 ? gn->smooth_scale : 1.f, c0, c1);
   }
-  return cudaGetLastError();
+  if (rc > 0) k_copy_probe_cols<<<gs, kThreads, 0, s>>>(h->N, L->snap, L->V, c1);
+  CUDA_TRY(cudaGetLastError());
+  return CGX_SUCCESS;
 }
 
 cgx_status cgx_gnn_set_probes(cgx_gnn *gn, int smooth_steps, int smooth_cols,
-                              float smooth_scale) {
+                              float smooth_scale, int residual_cols) {
   if (!gn) return fail(CGX_ERROR_INVALID_ARGUMENT, "network is NULL");
-  if (smooth_steps < 0 || smooth_cols < 0 || smooth_cols > S ||
-      !(smooth_scale > 0.f))
+  if (smooth_steps < 0 || smooth_cols < 0 || residual_cols < 0 ||
+      smooth_cols + residual_cols > S || !(smooth_scale > 0.f))
     return fail(CGX_ERROR_INVALID_ARGUMENT,
-                "need smooth_steps >= 0, 0 <= smooth_cols <= 8, smooth_scale > 0");
+                "need smooth_steps >= 0, smooth_cols, residual_cols >= 0 with "
+                "smooth_cols + residual_cols <= 8, smooth_scale > 0");
   gn->smooth_steps = smooth_steps;
   gn->smooth_cols = smooth_cols;
   gn->smooth_scale = smooth_scale;
+  gn->residual_cols = residual_cols;
+  return CGX_SUCCESS;
+}
+
+cgx_status cgx_learned_capture_residual(cgx_handle *h, int col) {
+  CGX_TRY(need_matrix(h));
+  if (!h->L) return fail(CGX_ERROR_INVALID_STATE, "call cgx_learned_setup first");
+  if (col < 0 || col >= S) return fail(CGX_ERROR_INVALID_ARGUMENT, "col must be in [0, 8)");
+  DeviceGuard guard(h->device);
+  CGX_TRY(learned_train_alloc(h));
+  Learned *L = h->L;
+  cudaStream_t s = h->stream;
+  CUDA_TRY(launch_spmv(h, h->vec[CGX_VECTOR_X],
+                       OpTrueResidual{h->vec[CGX_VECTOR_K], h->tmp,
+                                      ticket(h, kTicketTrue)}));
+  const int g = grid_stream(h, h->N);
+  k_snap_norm<<<g, kThreads, 0, s>>>(h->N, h->tmp, L->dis, h->partials,
+                                     ticket(h, kTicketDot), L->snap_scale);
+  k_snap_store<<<g, kThreads, 0, s>>>(h->N, h->tmp, L->dis, L->snap_scale, L->snap, col);
+  CUDA_TRY(cudaGetLastError());
+  L->snap_valid |= 1u << col;
   return CGX_SUCCESS;
 }
 
@@ -2143,7 +2183,7 @@ cgx_status cgx_gnn_loss_grad(cgx_gnn *gn, cgx_handle *h, const float *probes,
     CUDA_TRY(cudaMemcpyAsync(L->V, probes, sizeof(float) * h->N * S,
                              cudaMemcpyHostToDevice, s));
   else
-    CUDA_TRY(make_probes(gn, h, seed));
+    CGX_TRY(make_probes(gn, h, seed));
   CUDA_TRY(gnn_forward(h, gn->params, false));
   CUDA_TRY(gnn_backward(h, gn->params));
   if (loss)
@@ -2166,7 +2206,7 @@ cgx_status cgx_gnn_train_step(cgx_gnn *gn, cgx_handle *h, unsigned long long see
   CGX_TRY(learned_train_alloc(h));
   Learned *L = h->L;
   cudaStream_t s = h->stream;
-  CUDA_TRY(make_probes(gn, h, seed));
+  CGX_TRY(make_probes(gn, h, seed));
   CUDA_TRY(gnn_forward(h, gn->params, false));
   CUDA_TRY(gnn_backward(h, gn->params));
   gn->step++;

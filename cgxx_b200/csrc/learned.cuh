@@ -761,16 +761,56 @@ __global__ void k_adam(int n, float *__restrict__ p, float *__restrict__ m,
   }
 }
 
-// Smoothed probe columns: for the last `cols` of the S columns, V <- sc (V -
+// Smoothed probe columns: for columns [c0, c1) of the S columns, V <- sc (V -
 // om T) with T = Ahat V (one damped-Jacobi step on the Jacobi-scaled matrix;
 // sc is the column scale, applied once after the last step).
 __global__ void k_smooth_probes(int N, float *__restrict__ V,
                                 const float *__restrict__ T, float om, float sc,
-                                int cols) {
+                                int c0, int c1) {
+  const size_t n = (size_t)N * S;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const int c = (int)(i % S);
+    if (c >= c0 && c < c1) V[i] = sc * fmaf(-om, T[i], V[i]);
+  }
+}
+
+// Residual snapshot of the solver: s = sum_i (dis_i r_i)^2 over the FP64
+// residual r = b - A x; the last CTA stores the unit-RMS scale sqrt(N / s).
+__global__ void __launch_bounds__(kThreads)
+    k_snap_norm(int N, const double *__restrict__ r,
+                const double *__restrict__ dis, double *partials,
+                unsigned *ticket, double *scale) {
+  double a = 0.0;
+  for (int i = blockIdx.x * kThreads + threadIdx.x; i < N;
+       i += gridDim.x * kThreads) {
+    const double v = dis[i] * r[i];
+    a = fma(v, v, a);
+  }
+  double in[1] = {a}, out[1];
+  if (grid_reduce<1>(in, partials, ticket, out) && threadIdx.x == 0)
+    *scale = out[0] > 0.0 ? sqrt((double)N / out[0]) : 0.0;
+}
+
+// snap[i*S + col] = dis_i r_i * scale: the Jacobi-scaled residual with unit
+// RMS, the coordinates of the scaled system the probes live in.
+__global__ void k_snap_store(int N, const double *__restrict__ r,
+                             const double *__restrict__ dis,
+                             const double *__restrict__ scale,
+                             float *__restrict__ snap, int col) {
+  const double sc = *scale;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N;
+       i += gridDim.x * blockDim.x)
+    snap[(size_t)i * S + col] = (float)(dis[i] * r[i] * sc);
+}
+
+// V[:, c0:S) = snap[:, c0:S) (the residual probe columns).
+__global__ void k_copy_probe_cols(int N, const float *__restrict__ snap,
+                                  float *__restrict__ V, int c0) {
   const size_t n = (size_t)N * S;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x)
-    if ((int)(i % S) >= S - cols) V[i] = sc * fmaf(-om, T[i], V[i]);
+    if ((int)(i % S) >= c0) V[i] = snap[i];
 }
 
 // Rademacher probes from a counter-based hash: V[i*S+s] = +-1.

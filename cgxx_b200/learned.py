@@ -10,7 +10,9 @@ cgx_learned_*); this module orchestrates them through the C ABI:
       the Hutchinson loss ||(Ghat^T Ahat Ghat - I) V||^2 with Rademacher
       probes V (by default half of the 8 columns smoothed by 3 damped-Jacobi
       steps and scaled by 3, which weights the smooth end of the spectrum
-      that limits CG), then PCG on the held-out fields: learned G G^T
+      that limits CG; --residual-probes k takes k columns from residuals of
+      the solver's own plain Jacobi-CG iterates on each training matrix),
+      then PCG on the held-out fields: learned G G^T
       against Jacobi, both FP32-inner / FP64-refinement to a 1e-9 FP64 true
       residual, and plain FP64 Jacobi-CG.
 
@@ -133,6 +135,11 @@ def main(argv=None):
     t.add_argument("--smooth-steps", type=int, default=3)
     t.add_argument("--smooth-cols", type=int, default=4)
     t.add_argument("--smooth-scale", type=float, default=3.0)
+    t.add_argument("--residual-probes", type=int, default=0,
+                   help="probe columns taken from residuals of the solver's own "
+                        "plain Jacobi-CG iterates on each training matrix")
+    t.add_argument("--residual-its", default="5,10,20,40",
+                   help="iterations of the restarted solves before each snapshot")
     t.add_argument("--select", type=int, default=16,
                    help="held-out fields scored for checkpoint selection")
     t.add_argument("--seed", type=int, default=0)
@@ -189,7 +196,20 @@ def run_training(a):
     else:
         params = init_params(a.seed)
     net = cg.Gnn(0, params)
-    net.set_probes(a.smooth_steps, a.smooth_cols, a.smooth_scale)
+    net.set_probes(a.smooth_steps, a.smooth_cols, a.smooth_scale, a.residual_probes)
+    res_its = [int(t) for t in a.residual_its.split(",")][:a.residual_probes]
+    rhs = [np.random.default_rng(7 + k).uniform(-1.0, 1.0, fam.N) for k in range(4)]
+
+    def snapshots(k):
+        """Residual snapshots of training matrix k: plain Jacobi-CG from x = 0
+        on a random right-hand side, restarted after each res_its entry, with
+        r = b - A x captured after each part."""
+        h.jacobi_from_matrix()
+        h.set_vector("K", rhs[k % len(rhs)])
+        h.fill_vector("X", 0.0)
+        for j, its in enumerate(res_its):
+            h.solve(max_iterations=its, tolerance=1e-30)
+            h.learned_capture_residual(8 - a.residual_probes + j)
 
     def selection_score(gnn):
         its = []
@@ -222,6 +242,8 @@ def run_training(a):
             for k in order:
                 h.update_crs_values_ptr(tr_dev[k].data_ptr())
                 h.learned_setup()
+                if a.residual_probes:
+                    snapshots(int(k))
                 losses.append(net.train_step(h, seed=int(rng.integers(1 << 62)), lr=lr))
                 steps += 1
             score = selection_score(net)
@@ -260,6 +282,8 @@ def run_training(a):
                        "lr": a.lr, "eps": a.eps, "probes": 8,
                        "smooth_steps": a.smooth_steps, "smooth_cols": a.smooth_cols,
                        "smooth_scale": a.smooth_scale, "select": a.select,
+                       "residual_probes": a.residual_probes,
+                       "residual_its": res_its,
                        "loss": "||(Ghat^T Ahat Ghat - I) V||^2 / (N S), Rademacher V"},
             "log": log, "heldout": summary}
     if not a.eval_only:

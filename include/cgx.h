@@ -205,14 +205,23 @@ cgx_status cgx_learned_factor(cgx_handle *h, cgx_gnn *g, double eps);
  * each optional). */
 cgx_status cgx_learned_get_factor(cgx_handle *h, int *nnzL, float *ghat,
                                   int *rows, int *cols);
-/* Probe recipe of the network's training (no counterpart in the reference):
- * Rademacher columns from a seed; then the last `smooth_cols` of the 8
- * columns take `smooth_steps` damped-Jacobi steps V <- V - (2/3) Ahat V on
- * the Jacobi-scaled matrix and are multiplied by `smooth_scale`, which
- * weights the loss toward the smooth end of the spectrum. Default 0, 0, 1
- * (plain Rademacher probes). */
+/* Probe recipe of the network's training (no counterpart in the reference),
+ * for the 8 probe columns: the last `residual_cols` are the handle's
+ * residual snapshots (cgx_learned_capture_residual; they must exist for the
+ * current values); the `smooth_cols` before them are Rademacher columns
+ * that take `smooth_steps` damped-Jacobi steps V <- V - (2/3) Ahat V on the
+ * Jacobi-scaled matrix and are multiplied by `smooth_scale`; the rest are
+ * Rademacher columns from the seed. Both kinds weight the loss toward the
+ * smooth end of the spectrum that limits CG. Default 0, 0, 1, 0 (plain
+ * Rademacher probes). */
 cgx_status cgx_gnn_set_probes(cgx_gnn *g, int smooth_steps, int smooth_cols,
-                              float smooth_scale);
+                              float smooth_scale, int residual_cols);
+/* Residual snapshot for the probe recipe (no counterpart in the reference):
+ * r = k - A x of the current K and X in FP64 (x typically an iterate of a
+ * solve the caller ran), Jacobi-scaled (D^-1/2 r) and normalized to unit
+ * RMS, stored as probe column `col` (0..7) of the handle's learned state.
+ * Snapshots are dropped when cgx_learned_setup takes new values. */
+cgx_status cgx_learned_capture_residual(cgx_handle *h, int col);
 /* Hutchinson loss ||(Ghat^T Ahat Ghat - I) V||_F^2 / (N S) for S = 8 probe
  * columns (probes: N*8 floats, node-major, or NULL for the network's probe
  * recipe from `seed`) and its gradient w.r.t. the parameters (grad may be

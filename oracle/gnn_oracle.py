@@ -138,6 +138,14 @@ def smooth_probes(g: Graph, V, steps, cols, scale, omega=2.0 / 3.0):
     return V.numpy()
 
 
+def residual_probe(g: Graph, r):
+    """A residual snapshot as a probe column: the Jacobi-scaled residual
+    D^-1/2 r normalized to unit RMS (computed in FP64, stored in FP32)."""
+    v = np.asarray(r, np.float64) / np.sqrt(g.d)
+    s = float(v @ v)
+    return (v * np.sqrt(g.N / s) if s > 0 else 0.0 * v).astype(np.float32)
+
+
 def forward(g: Graph, flat):
     """Returns (gdiag[N], goff[n_lower]) in lower-pattern order (row-major,
     storage order within a row) as float32 tensors with autograd."""

@@ -58,7 +58,8 @@ def test_default_options_match_reference_defaults():
 
 def test_errors_are_statuses():
     lib = cg.load()
-    assert lib.cgx_gnn_set_probes(None, 0, 0, 1.0) == 1
+    assert lib.cgx_gnn_set_probes(None, 0, 0, 1.0, 0) == 1
+    assert lib.cgx_learned_capture_residual(None, 0) == 1
     with pytest.raises(cg.CgxError) as e:
         _lib.check(lib.cgx_create(C.byref(C.c_void_p()), -1))
     assert e.value.status == 1

@@ -129,6 +129,41 @@ def test_probe_recipe_matches_oracle():
     net.close()
 
 
+def test_residual_probes_match_oracle():
+    """Residual snapshots of the solver's own iterates as probe columns: the
+    device's capture (D^-1/2 (k - A x), unit RMS) equals the oracle's, so the
+    loss from the recipe matches the loss from explicit probes."""
+    A = G.diffusion3d(12, 7, seed=6)
+    h = _setup(A)
+    b, _ = G.rhs_for(A, seed=3)
+    h.upload_jacobi(1.0 / A.diagonal())
+    h.set_vector("K", b)
+    h.fill_vector("X", 0.0)
+    gr = GO.Graph(A.ptr, A.index, A.value)
+    cols = []
+    for c, its in ((6, 3), (7, 7)):
+        h.solve(max_iterations=its, tolerance=1e-30)
+        h.learned_capture_residual(c)
+        x = h.get_vector("X")
+        cols.append(GO.residual_probe(gr, b - A.matvec(x)))
+    net = cg.Gnn(0, _params(3))
+    net.set_probes(residual_cols=2)
+    seed = 99
+    l_dev, g_dev = net.loss_grad(h, seed=seed)
+    V = GO.rademacher(A.N, seed)
+    V[:, 6], V[:, 7] = cols[0], cols[1]
+    l_ref, g_ref = net.loss_grad(h, probes=V)
+    assert abs(l_dev - l_ref) <= 1e-5 * abs(l_ref)
+    assert np.linalg.norm(g_dev - g_ref) <= 1e-4 * np.linalg.norm(g_ref)
+    # New values drop the snapshots: the recipe then refuses to run.
+    h.update_crs_values(A.value * 2.0)
+    h.learned_setup()
+    with pytest.raises(cg.CgxError):
+        net.loss_grad(h, seed=seed)
+    h.close()
+    net.close()
+
+
 def test_training_lowers_the_loss():
     fam = G.Diffusion7Family(12)
     rng = np.random.default_rng(0)
