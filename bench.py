@@ -384,15 +384,24 @@ def our_arm(args, world, rank, local):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1), r
 
+    def accuracy():
+        """FP64 true relative residual of the current X, and its relative
+        error against the exact solution x* of b = A x* (FP64, on the CPU)."""
+        xv = h.get_vector("X")
+        return {"true_residual": float(np.linalg.norm(b - A.matvec(xv)) / np.linalg.norm(b)),
+                "rel_error_vs_exact": float(np.linalg.norm(xv - xs) / np.linalg.norm(xs))}
+
     side = {args.path: {"ms": ms, "iterations": res["iterations"],
                         "outer_iterations": res["outer_iterations"],
-                        "fell_back": bool(res["fell_back"])}}
+                        "fell_back": bool(res["fell_back"]),
+                        "true_residual": true_rel, "rel_error_vs_exact": err_vs_exact}}
     for p in others:
         runs = [timed(p) for _ in range(2)]
         side[p] = {"ms": statistics.median(t for t, _ in runs),
                    "iterations": runs[-1][1]["iterations"],
                    "outer_iterations": runs[-1][1]["outer_iterations"],
                    "fell_back": bool(runs[-1][1]["fell_back"])}
+        side[p].update(accuracy())
     # Learned path: network set-up + inference alone.
     fe0 = torch.cuda.Event(enable_timing=True)
     fe1 = torch.cuda.Event(enable_timing=True)
