@@ -1794,7 +1794,7 @@ cudaError_t gnn_forward(cgx_handle *h, const float *P, bool scaled) {
   // Inference (scaled) keeps no pre-activations or aggregates: only the
   // backward pass needs them.
   const bool keep = !scaled;
-  k_embed<<<grid_for(h, (size_t)N * W), kThreads, 0, s>>>(
+  k_embed<<<grid_for(h, (size_t)N), kThreads, 0, s>>>(
       N, L->feat, P, L->h[0], keep ? L->pre[0] : nullptr);
   const int groups = (N + 15) / 16;
   const int lgrid = std::max(

@@ -211,16 +211,29 @@ __device__ __forceinline__ float relu(float x) { return x > 0.f ? x : 0.f; }
 __global__ void k_embed(int N, const float *__restrict__ feat,
                         const float *__restrict__ P, __nv_bfloat16 *__restrict__ h,
                         float *__restrict__ pre) {
-  const int total = N * W;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total;
-       t += gridDim.x * blockDim.x) {
-    const int i = t / W, f = t % W;
-    float s = P[OFF_BIN + f];
+  // One thread per node: W_in and b_in (contiguous in P) from shared memory,
+  // the node's 4 features in one 16-byte load, its 32 outputs in four
+  // 16-byte stores.
+  __shared__ float sW[W * NIN + W];
+  for (int t = threadIdx.x; t < W * NIN + W; t += blockDim.x) sW[t] = P[OFF_WIN + t];
+  __syncthreads();
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N;
+       i += gridDim.x * blockDim.x) {
+    const float4 f4 = *reinterpret_cast<const float4 *>(feat + (size_t)i * NIN);
+    const float fv[NIN] = {f4.x, f4.y, f4.z, f4.w};
+    uint4 out[W / 8];
+    __nv_bfloat16 *ob = reinterpret_cast<__nv_bfloat16 *>(out);
 #pragma unroll
-    for (int k = 0; k < NIN; k++)
-      s = fmaf(P[OFF_WIN + f * NIN + k], feat[i * NIN + k], s);
-    if (pre) pre[t] = s;
-    h[t] = __float2bfloat16_rn(relu(s));
+    for (int f = 0; f < W; f++) {
+      float s = sW[W * NIN + f];
+#pragma unroll
+      for (int k = 0; k < NIN; k++) s = fmaf(sW[f * NIN + k], fv[k], s);
+      if (pre) pre[(size_t)i * W + f] = s;
+      ob[f] = __float2bfloat16_rn(relu(s));
+    }
+    uint4 *dst = reinterpret_cast<uint4 *>(h + (size_t)i * W);
+#pragma unroll
+    for (int q = 0; q < W / 8; q++) dst[q] = out[q];
   }
 }
 
@@ -341,21 +354,30 @@ __global__ void __launch_bounds__(32 * kLayerWarps)
         mma_bf16_16816(acc[nt], a, b);
       }
     }
-    // Epilogue: rows g and g+8, columns nt*8 + 2tq + {0,1}.
+    // Epilogue: rows g and g+8, columns nt*8 + 2tq + {0,1}. The new h
+    // replaces h_i in the staging rows (each element is read and written by
+    // the lane that owns it), then the warp stores its 16 rows as 16-byte
+    // chunks.
 #pragma unroll
     for (int nt = 0; nt < 4; nt++)
 #pragma unroll
       for (int q = 0; q < 4; q++) {
         const int r = g + (q >= 2 ? 8 : 0);
         const int col = nt * 8 + 2 * tq + (q & 1);
-        const int i = base + r;
-        if (i < N) {
-          const float pre = acc[nt][q] + sB[col];
-          if (pre_out) pre_out[(size_t)i * W + col] = pre;
-          const float hv = __bfloat162float(sX[warp][r][col]) + relu(pre);
-          hout[(size_t)i * W + col] = __float2bfloat16_rn(hv);
-        }
+        const float pre = acc[nt][q] + sB[col];
+        if (pre_out && base + r < N) pre_out[(size_t)(base + r) * W + col] = pre;
+        const float hv = __bfloat162float(sX[warp][r][col]) + relu(pre);
+        sX[warp][r][col] = __float2bfloat16_rn(hv);
       }
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+      const int task = lane + 32 * q;
+      const int r = task >> 2, c4 = task & 3;
+      if (base + r < N)
+        reinterpret_cast<uint4 *>(hout)[(size_t)(base + r) * (W / 8) + c4] =
+            *reinterpret_cast<const uint4 *>(&sX[warp][r][8 * c4]);
+    }
     __syncwarp();
   }
 }
@@ -419,15 +441,14 @@ __global__ void k_assemble(int nnzL, const int *__restrict__ grow,
       v = fabsf(ahat[g2a[e]]) * (1.f + o[i * NOUT + 0] + uv);
     }
     ghat[e] = v;
-    if (gs) {
+    if (sgv) {  // the SELL-U copies of G and G^T (BF16)
+      const __nv_bfloat16 bv = __float2bfloat16_rn((float)(dis[i] * (double)v));
+      sgv[g2sg[e]] = bv;
+      stv[t2st[g2t[e]]] = bv;
+    } else if (gs) {  // FP32 CRS copies when the SELL-U layouts do not fit
       const float sv = (float)(dis[i] * (double)v);
       gs[e] = sv;
       gts[g2t[e]] = sv;
-      if (sgv) {  // the SELL-U copies of G and G^T
-        const __nv_bfloat16 bv = __float2bfloat16_rn(sv);
-        sgv[g2sg[e]] = bv;
-        stv[t2st[g2t[e]]] = bv;
-      }
     }
   }
 }
