@@ -1312,15 +1312,16 @@ static cgx_status ensure_f32(cgx_handle *h) {
   k_to_f32<<<grid_stream(h, N), kThreads, 0, h->stream>>>((size_t)N, h->C,
                                                           h->C32);
   CUDA_TRY(cudaGetLastError());
-  // SELL-U copy of A (pattern once per matrix, values on every refresh).
+  // SELL-U copy of A: the pattern once per matrix, the value array once it
+  // exists, the values on every refresh.
   if (!h->sa_tried) {
     h->sa_tried = true;
     CGX_TRY(build_sellu(h, h->ptr, h->index, (size_t)h->nz, h->sa));
-    if (h->sa.ok) {
-      CUDA_TRY(cudaMalloc(&h->sa_val, sizeof(float) * (h->sa.slots + kPad)));
-      CUDA_TRY(cudaMemsetAsync(h->sa_val, 0, sizeof(float) * (h->sa.slots + kPad),
-                               h->stream));
-    }
+  }
+  if (h->sa.ok && !h->sa_val) {
+    CUDA_TRY(cudaMalloc(&h->sa_val, sizeof(float) * (h->sa.slots + kPad)));
+    CUDA_TRY(cudaMemsetAsync(h->sa_val, 0, sizeof(float) * (h->sa.slots + kPad),
+                             h->stream));
   }
   if (h->sa.ok) {
     k_sellu_scatter<double, float><<<grid_stream(h, h->nz), kThreads, 0, h->stream>>>(
