@@ -52,6 +52,9 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--n", type=int, default=160, help="grid edge (default 160)")
+    ap.add_argument("--stencil", type=int, choices=[7, 27], default=7)
+    ap.add_argument("--graph", type=int, default=0,
+                    help="points of a random geometric graph instead of the grid")
     ap.add_argument("--path", choices=["learned", "mixed", "plain"], default="learned")
     ap.add_argument("--weights", default=os.path.join(REPO, "cgxx_b200", "weights",
                                                        "diffusion7.gnn"))
@@ -104,18 +107,33 @@ def max_over_ranks(world, v):
 # ---------------------------------------------------------------------------
 # Workload
 
-def workload(n):
+def workload(n, stencil=7, graph=0):
+    """The 3D diffusion matrix on an n^3 grid (7- or 27-point stencil), or
+    with graph > 0 the random geometric graph Laplacian on that many points,
+    and b = A x* for a seeded x*."""
     from cgxx_b200 import generators as G
-    A = G.diffusion3d(n, stencil=7, sigma=1.0, corr_len=8.0, seed=2024)
+    if graph:
+        A = G.geometric_graph(graph, mean_degree=12.0, seed=2024)
+    else:
+        A = G.diffusion3d(n, stencil=stencil, sigma=1.0, corr_len=8.0, seed=2024)
     b, xs = G.rhs_for(A, seed=7)
     return A, b, xs
 
 
+def workload_name(args):
+    if args.graph:
+        return f"geometric-graph-{args.graph}-deg12"
+    return f"diffusion3d-{args.stencil}pt-{args.n}^3"
+
+
 def workload_config(args, A):
+    field = ("random geometric graph, uniform points in the unit cube, mean degree 12, "
+             "w = exp(-d/r), L + 1e-3 I, seed 2024" if args.graph else
+             "exp(GRF sigma=1, corr_len=8 cells), seed 2024")
     return {
-        "workload": f"diffusion3d-7pt-{args.n}^3",
+        "workload": workload_name(args),
         "N": A.N, "nnz": A.nz, "format": "CRS", "preconditioner": "jacobi",
-        "path": args.path, "field": "exp(GRF sigma=1, corr_len=8 cells), seed 2024",
+        "path": args.path, "field": field,
         "rhs": "A x*, x* ~ U[-1,1] seed 7", "tolerance": args.tol,
         "max_iterations": args.max_iter, "l2": "inputs larger than L2 (no flush)",
         "parallelism": "replicas" if args.gpus > 1 else "single GPU",
@@ -184,9 +202,9 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # Reference CPU implementation (oracle/_ref, built from the reference sources)
 
-def mtx_cache_path(A, n):
+def mtx_cache_path(A, name):
     os.makedirs(CACHE, exist_ok=True)
-    path = os.path.join(CACHE, f"diffusion7_{n}.mtx")
+    path = os.path.join(CACHE, name.replace("^", "_") + ".mtx")
     if not os.path.exists(path):
         tmp = path + f".tmp{os.getpid()}"
         from cgxx_b200 import generators as G
@@ -195,12 +213,12 @@ def mtx_cache_path(A, n):
     return path
 
 
-def run_reference(A, b, n, reps, max_iter, tol, threads):
+def run_reference(A, b, name, reps, max_iter, tol, threads):
     """Runs the reference's OpenMP CG in-process harness on the workload with
     right-hand side b. Returns the list of per-repetition solve times (s) and
     the iteration counts."""
     from oracle import oracle as O
-    path = mtx_cache_path(A, n)
+    path = mtx_cache_path(A, name)
     env = {"CG_MAX_ITER": str(max_iter), "CG_TOLERANCE": repr(tol),
            "CG_MATRIX_FORMAT": "CRS", "CG_PRECONDITIONER": "jacobi",
            "OMP_NUM_THREADS": str(threads), "OMP_PROC_BIND": "spread"}
@@ -223,15 +241,15 @@ def reference_arm(args, world, rank):
         print(json.dumps({"impl": "reference", "unavailable":
                           "oracle/_ref/ref_harness_omp was not built (reference sources absent)"}))
         return
-    A, b, _ = workload(args.n)
+    A, b, _ = workload(args.n, args.stencil, args.graph)
     threads = host_threads()
     # Warm-up repetitions are full solves; they also give the iteration count
     # and the time of one full solve.
-    wt, witers, _ = run_reference(A, b, args.n, max(1, args.warmup), args.max_iter,
+    wt, witers, _ = run_reference(A, b, workload_name(args), max(1, args.warmup), args.max_iter,
                                   args.tol, threads)
     full_iters, full_s = witers[-1], min(wt)
     if full_s * args.steps <= 240.0:
-        times, iters, _ = run_reference(A, b, args.n, args.steps, args.max_iter, args.tol,
+        times, iters, _ = run_reference(A, b, workload_name(args), args.steps, args.max_iter, args.tol,
                                         threads)
         ms = 1e3 * sum(times) / len(times)
         sample = (f"{args.steps} full solves ({iters[-1]} iterations) by the reference's "
@@ -240,7 +258,7 @@ def reference_arm(args, world, rank):
         # Bounded sample: each step runs `cap` iterations; the time is scaled
         # to the full iteration count.
         cap = max(10, int(full_iters * 240.0 / (full_s * args.steps)))
-        times, iters, _ = run_reference(A, b, args.n, args.steps, cap, args.tol, threads)
+        times, iters, _ = run_reference(A, b, workload_name(args), args.steps, cap, args.tol, threads)
         ms = 1e3 * (sum(times) / len(times)) * full_iters / iters[-1]
         sample = (f"{args.steps} solves capped at {iters[-1]} iterations (CG_MAX_ITER), "
                   f"scaled to the full {full_iters}; CGOpenMP, OMP_NUM_THREADS={threads}")
@@ -262,7 +280,15 @@ def reference_arm(args, world, rank):
 # ---------------------------------------------------------------------------
 # Our arm
 
-def read_traffic_profile(name):
+def read_traffic_profile(name, args):
+    """ncu DRAM traffic per launch committed under profiles/ for the default
+    workload (7-point 160^3); None for other workloads."""
+    if workload_name(args) != "diffusion3d-7pt-160^3":
+        return None
+    return _read_profile(name)
+
+
+def _read_profile(name):
     p = os.path.join(REPO, "profiles", name)
     try:
         with open(p) as f:
@@ -299,6 +325,8 @@ def load_network(args):
     present, else the untrained initialisation (reported as such)."""
     from cgxx_b200 import learned as LRN
     path = args.weights
+    if path == "init":
+        return LRN.init_params(0), {"weights": "untrained initialisation (--weights init)"}
     if path and os.path.exists(path):
         params, head = LRN.load_weights(path)
         return params, {"weights": os.path.relpath(path, REPO),
@@ -312,7 +340,7 @@ def our_arm(args, world, rank, local):
 
     import cgxx_b200 as cg
 
-    A, b, xs = workload(args.n)
+    A, b, xs = workload(args.n, args.stencil, args.graph)
     Cd = 1.0 / A.diagonal()
     N, nnz = A.N, A.nz
     dev = local if world > 1 else 0
@@ -440,7 +468,7 @@ def our_arm(args, world, rank, local):
                  "kernel": "k_crs<double, OpPcgQ>: q = A p fused with <p,q> (FP64 CRS)",
                  "algorithmic_bytes": fp64_spmv_bytes, "peak_kind": peak_kind}
     fp64_roof["frac"] = fp64_roof["achieved"] / peak
-    prof = read_traffic_profile("spmv_crs_fp64_diffusion7_160.json")
+    prof = read_traffic_profile("spmv_crs_fp64_diffusion7_160.json", args)
     fp64_roof["traffic"] = prof.get("dram_bytes_per_launch") if prof else None
     if args.path == "plain":
         roof = fp64_roof
@@ -460,7 +488,7 @@ def our_arm(args, world, rank, local):
                 "peak": peak, "unit": "GB/s", "kernel": kname,
                 "algorithmic_bytes": fp32_spmv_bytes, "peak_kind": peak_kind}
         roof["frac"] = roof["achieved"] / peak
-        prof32 = read_traffic_profile("spmv_sellu_fp32_diffusion7_160.json")
+        prof32 = read_traffic_profile("spmv_sellu_fp32_diffusion7_160.json", args)
         roof["traffic"] = prof32.get("dram_bytes_per_launch") if prof32 else None
 
     # End to end through the public C ABI: pinned host inputs uploaded every
@@ -554,7 +582,7 @@ def cpu_baseline(A, b, args, full_iters):
     threads = host_threads()
     sample = 100
     try:
-        times, iters, _ = run_reference(A, b, args.n, 2, sample, args.tol, threads)
+        times, iters, _ = run_reference(A, b, workload_name(args), 2, sample, args.tol, threads)
     except Exception as e:  # pragma: no cover - reported, not fatal
         return {"value": None, "error": str(e)[:200]}
     t = min(times)

@@ -452,11 +452,12 @@ static cudaError_t launch_pcg_setup(cgx_handle *h, bool jacobi) {
 
 // q = A p in FP32 with <p,q> (inner solves), compact indices when they fit.
 // k_sellu over one wave of CTAs (as many as fit on the SMs at once), fewer
-// when the slice pairs run out; chunks of 4 slots when no slice is wider.
-template <typename VT, int U, typename Op>
+// when the slice pairs run out; chunks of 4 slots when no slice is wider,
+// and the uniform-only kernel when every slice is uniform.
+template <typename VT, int U, bool ALL_UNIFORM, typename Op>
 static cudaError_t launch_sellu_u(cgx_handle *h, SellUView<VT> A, const float *x,
                                   Op op) {
-  auto kern = k_sellu<VT, U, Op>;
+  auto kern = k_sellu<VT, U, ALL_UNIFORM, Op>;
   int per_sm = 0;
   cudaError_t e =
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, 0);
@@ -472,8 +473,12 @@ template <typename VT, typename Op>
 static cudaError_t launch_sellu(cgx_handle *h, const SellU &S, const VT *val,
                                 const float *x, Op op) {
   const SellUView<VT> A{S.meta, S.off, val, h->N};
-  return S.max_width <= 4 ? launch_sellu_u<VT, 4>(h, A, x, op)
-                          : launch_sellu_u<VT, 8>(h, A, x, op);
+  const bool all = S.uniform == (long long)((h->N + 31) / 32);
+  if (S.max_width <= 4)
+    return all ? launch_sellu_u<VT, 4, true>(h, A, x, op)
+               : launch_sellu_u<VT, 4, false>(h, A, x, op);
+  return all ? launch_sellu_u<VT, 8, true>(h, A, x, op)
+             : launch_sellu_u<VT, 8, false>(h, A, x, op);
 }
 
 static cudaError_t launch_inner_q(cgx_handle *h) {

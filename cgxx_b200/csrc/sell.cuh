@@ -79,8 +79,9 @@ __device__ __forceinline__ float4 load_group(const __nv_bfloat16 *p) {
 // unconditional: groups and gathers past the slice's width re-read its last
 // ones (L1 hits) and are masked out, so every value load and gather of a
 // chunk is issued before the first multiply-add (predicated loads would
-// split the chunk into branches and serialize the round trips). Per-row
-// slices take a plain loop with a per-entry offset load.
+// split the chunk into branches and serialize the round trips). Steps whose
+// slices are all per-row take the same chunks with per-entry offset loads;
+// a step that mixes both kinds takes a plain loop.
 template <typename VT>
 struct SellUView {
   const int4 *meta;  // per slice {vb (groups), w (slots), ob, uniform}
@@ -89,7 +90,10 @@ struct SellUView {
   int N;
 };
 
-template <typename VT, int U, typename Op>
+// ALL_UNIFORM: the layout has no per-row slice, and its instantiation
+// leaves out the chunked per-row path (measured: carrying it costs the
+// uniform kernels 1-3 %).
+template <typename VT, int U, bool ALL_UNIFORM, typename Op>
 __global__ void __launch_bounds__(kThreads)
     k_sellu(SellUView<VT> A, const float *__restrict__ x, Op op, CgState *st,
             double *partials) {
@@ -109,7 +113,7 @@ __global__ void __launch_bounds__(kThreads)
   for (; s0 < nslices; s0 += stride) {
     const int4 mn = meta_of(s0 + stride);
     int vb[SPW], w[SPW], ob[SPW], uni[SPW], row[SPW];
-    bool fast = true;
+    bool fast = true, perrow = true;
     int wmax = 0;
 #pragma unroll
     for (int q = 0; q < SPW; q++) {
@@ -119,6 +123,7 @@ __global__ void __launch_bounds__(kThreads)
       uni[q] = __shfl_sync(0xffffffffu, ml.w, q);
       row[q] = ((s0 + q) << 5) + lane;
       fast = fast && (uni[q] || w[q] == 0);
+      perrow = !ALL_UNIFORM && perrow && (!uni[q] || w[q] == 0);
       wmax = max(wmax, w[q]);
     }
     typename Op::Pre pre[SPW];
@@ -155,6 +160,47 @@ __global__ void __launch_bounds__(kThreads)
             b[q][u] = __ldg(&x[min((unsigned)(row[q] + o), nmax)]);
           }
         }
+#pragma unroll
+        for (int q = 0; q < SPW; q++)
+#pragma unroll
+          for (int g = 0; g < NG; g++) {
+            const float4 v = (k0 >> 2) + g < ng[q] ? a[q][g] : make_float4(0.f, 0.f, 0.f, 0.f);
+            sum[q] = fmaf(v.x, b[q][4 * g + 0], sum[q]);
+            sum[q] = fmaf(v.y, b[q][4 * g + 1], sum[q]);
+            sum[q] = fmaf(v.z, b[q][4 * g + 2], sum[q]);
+            sum[q] = fmaf(v.w, b[q][4 * g + 3], sum[q]);
+          }
+      }
+    } else if (perrow) {
+      // Per-row slices, the same chunks: a slot's offset is the lane's own
+      // (one coalesced load per slot, clamped to the slice's last slot), and
+      // all offset loads of a chunk are issued before its gathers.
+      int ng[SPW];
+#pragma unroll
+      for (int q = 0; q < SPW; q++) ng[q] = (w[q] + 3) >> 2;
+      const unsigned nmax = (unsigned)(A.N - 1);
+      for (int k0 = 0; k0 < wmax; k0 += U) {
+        float4 a[SPW][NG];
+        int o[SPW][U];
+        float b[SPW][U];
+#pragma unroll
+        for (int q = 0; q < SPW; q++) {
+#pragma unroll
+          for (int g = 0; g < NG; g++) {
+            const int gi = (k0 >> 2) + g;
+            a[q][g] = load_group(A.val + ((((vb[q] + min(gi, max(ng[q] - 1, 0))) << 5) + lane) << 2));
+          }
+#pragma unroll
+          for (int u = 0; u < U; u++) {
+            const int kk = min(k0 + u, max(w[q] - 1, 0));
+            o[q][u] = w[q] > 0 ? __ldg(&A.off[ob[q] + (kk << 5) + lane]) : 0;
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < SPW; q++)
+#pragma unroll
+          for (int u = 0; u < U; u++)
+            b[q][u] = __ldg(&x[min((unsigned)(row[q] + o[q][u]), nmax)]);
 #pragma unroll
         for (int q = 0; q < SPW; q++)
 #pragma unroll

@@ -207,11 +207,27 @@ def diffusion3d(n, stencil=7, sigma=1.0, corr_len=8.0, seed=0, coeff=None):
 # ---------------------------------------------------------------------------
 # Random geometric graph Laplacian
 
+def _morton_order(pts, bits=10):
+    """Permutation that sorts points in [0,1)^3 along a Z-order (Morton)
+    curve of 2^bits cells per axis."""
+    q = np.minimum((pts * (1 << bits)).astype(np.uint64), (1 << bits) - 1)
+    code = np.zeros(len(pts), np.uint64)
+    for b in range(bits):
+        for a in range(3):
+            code |= ((q[:, a] >> np.uint64(b)) & np.uint64(1)) << np.uint64(3 * b + a)
+    return np.argsort(code, kind="stable")
+
+
 def geometric_graph(npts, mean_degree=12.0, seed=0, shift=1e-3):
+    """Random geometric graph Laplacian: npts uniform points in the unit
+    cube, numbered along a Morton curve (neighbouring points get nearby
+    numbers), edges between points closer than r with r set for the mean
+    degree, weights exp(-d/r), plus shift * I."""
     from scipy.spatial import cKDTree
 
     rng = np.random.default_rng(seed)
     pts = rng.random((npts, 3))
+    pts = pts[_morton_order(pts)]
     r = (3.0 * mean_degree / (4.0 * np.pi * npts)) ** (1.0 / 3.0)
     pairs = cKDTree(pts).query_pairs(r, output_type="ndarray").astype(np.int64)
     i, j = pairs[:, 0], pairs[:, 1]

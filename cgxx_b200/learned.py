@@ -3,6 +3,10 @@
 The network and its training run on the GPU in libcgb200 (cgx_gnn_*,
 cgx_learned_*); this module orchestrates them through the C ABI:
 
+  python -m cgxx_b200.learned train --family graph --out cgxx_b200/weights/graph12.gnn
+      256 seeded random geometric graphs of 200k points (mean degree 12),
+      16 held-out, the same loss, probes and selection.
+
   python -m cgxx_b200.learned train --out cgxx_b200/weights/diffusion7.gnn
       512 seeded training fields and 64 held-out fields on a 96^3 grid
       (7-point diffusion, coefficient exp(g), g a Gaussian random field with
@@ -126,9 +130,13 @@ def main(argv=None):
     ap = argparse.ArgumentParser()
     sub = ap.add_subparsers(dest="cmd", required=True)
     t = sub.add_parser("train")
-    t.add_argument("--n", type=int, default=96)
-    t.add_argument("--train", type=int, default=512)
-    t.add_argument("--heldout", type=int, default=64)
+    t.add_argument("--family", choices=["diffusion7", "graph"], default="diffusion7")
+    t.add_argument("--n", type=int, default=96, help="grid edge (diffusion7)")
+    t.add_argument("--points", type=int, default=200000, help="points per graph (graph)")
+    t.add_argument("--train", type=int, default=None,
+                   help="training matrices (default 512 fields, 256 graphs)")
+    t.add_argument("--heldout", type=int, default=None,
+                   help="held-out matrices (default 64 fields, 16 graphs)")
     t.add_argument("--epochs", type=int, default=4)
     t.add_argument("--lr", type=float, default=2e-3)
     t.add_argument("--eps", type=float, default=1e-4)
@@ -149,7 +157,15 @@ def main(argv=None):
     t.add_argument("--eval-only", action="store_true")
     a = ap.parse_args(argv)
     if a.cmd == "train":
-        run_training(a)
+        graph = a.family == "graph"
+        if a.train is None:
+            a.train = 256 if graph else 512
+        if a.heldout is None:
+            a.heldout = 16 if graph else 64
+        if graph:
+            run_graph_training(a)
+        else:
+            run_training(a)
 
 
 def init_params(seed=0):
@@ -283,6 +299,133 @@ def run_training(a):
                        "smooth_steps": a.smooth_steps, "smooth_cols": a.smooth_cols,
                        "smooth_scale": a.smooth_scale, "select": a.select,
                        "residual_probes": a.residual_probes,
+                       "residual_its": res_its,
+                       "loss": "||(Ghat^T Ahat Ghat - I) V||^2 / (N S), Rademacher V"},
+            "log": log, "heldout": summary}
+    if not a.eval_only:
+        save_weights(a.out, params, meta)
+    if a.report:
+        with open(a.report, "w") as f:
+            json.dump({"meta": meta, "per_matrix": res}, f, indent=1)
+    print(json.dumps({"summary": summary, "train_seconds": train_s, "steps": steps}))
+
+
+def _graph_arrays(args):
+    npts, seed = args
+    from cgxx_b200 import generators as G
+    A = G.geometric_graph(npts, mean_degree=12.0, seed=seed)
+    return A.ptr, A.index, A.value
+
+
+def _arrays_diag_inv(ptr, index, value):
+    rows = np.repeat(np.arange(len(ptr) - 1), np.diff(ptr))
+    d = np.zeros(len(ptr) - 1)
+    m = rows == index
+    d[rows[m]] = value[m]
+    return 1.0 / d
+
+
+def run_graph_training(a):
+    """The irregular family: random geometric graph Laplacians (a.points
+    uniform points in the unit cube, mean degree 12, w = exp(-d/r), L + 1e-3 I),
+    one seeded graph per training step. Every graph has its own pattern, so
+    each step uploads it and runs a fresh set-up; the graphs of an epoch are
+    generated by a spawn process pool (created before any CUDA work)
+    while the GPU trains on the previous batch."""
+    import multiprocessing as mp
+    t0 = time.time()
+    tr_seeds = [300000 + 1000 * a.seed + k for k in range(a.train)]
+    ho_seeds = [700000 + 1000 * a.seed + k for k in range(a.heldout)]
+    pool = mp.get_context("spawn").Pool(a.workers)
+    ho = pool.map(_graph_arrays, [(a.points, sd) for sd in ho_seeds], chunksize=1)
+    gen_s = time.time() - t0
+
+    import cgxx_b200 as cg
+    from cgxx_b200 import generators as G
+    h = cg.Handle(0)
+    if a.eval_only:
+        params, head = load_weights(a.out)
+    else:
+        params = init_params(a.seed)
+    net = cg.Gnn(0, params)
+    net.set_probes(a.smooth_steps, a.smooth_cols, a.smooth_scale, a.residual_probes)
+    res_its = [int(t) for t in a.residual_its.split(",")][:a.residual_probes]
+
+    def load(arrs, k):
+        ptr, index, value = arrs
+        h.upload_crs(ptr, index, value)
+        h.upload_jacobi(_arrays_diag_inv(ptr, index, value))
+        b, _ = G.rhs_for(G.Crs(len(ptr) - 1, ptr, index, value), seed=k)
+        h.set_vector("K", b)
+        h.learned_setup()
+        return b
+
+    def selection_score(gnn):
+        its = []
+        for k, arrs in enumerate(ho[:a.select]):
+            load(arrs, k)
+            h.learned_factor(gnn, a.eps)
+            h.fill_vector("X", 0.0)
+            r = h.solve(max_iterations=20000, tolerance=1e-9,
+                        preconditioner=cg.PRECOND_LEARNED, precision=cg.PRECISION_MIXED)
+            its.append(r["iterations"] if r["converged"] else 10 ** 9)
+        return float(np.median(its))
+
+    log = []
+    t1 = time.time()
+    steps = 0
+    selected = 0
+    if not a.eval_only:
+        best = (selection_score(net), 0, net.get_params())
+        log.append({"epoch": -1, "selection_median_iterations": best[0]})
+        print(json.dumps(log[-1]), flush=True)
+        rng = np.random.default_rng(a.seed)
+        for ep in range(a.epochs):
+            order = [tr_seeds[k] for k in rng.permutation(len(tr_seeds))]
+            losses = []
+            lr = a.lr * (0.5 ** ep)
+            for arrs in pool.imap(_graph_arrays, [(a.points, sd) for sd in order], chunksize=1):
+                load(arrs, steps)
+                if a.residual_probes:
+                    h.fill_vector("X", 0.0)
+                    for j, its in enumerate(res_its):
+                        h.solve(max_iterations=its, tolerance=1e-30)
+                        h.learned_capture_residual(8 - a.residual_probes + j)
+                losses.append(net.train_step(h, seed=int(rng.integers(1 << 62)), lr=lr))
+                steps += 1
+            score = selection_score(net)
+            log.append({"epoch": ep, "lr": lr, "mean_loss": float(np.mean(losses)),
+                        "selection_median_iterations": score})
+            print(json.dumps(log[-1]), flush=True)
+            if score < best[0]:
+                best = (score, ep + 1, net.get_params())
+        selected = best[1]
+        net.set_params(best[2])
+    pool.close()
+    train_s = time.time() - t1
+    params = net.get_params()
+
+    res = []
+    init_net = cg.Gnn(0, init_params(a.seed))
+    for k, arrs in enumerate(ho):
+        b = load(arrs, k)
+        r = solve_pair(h, arrs[0], arrs[1], arrs[2], b, True, net, a.eps)
+        h.learned_setup()
+        h.learned_factor(init_net, a.eps)
+        h.fill_vector("X", 0.0)
+        ri = h.solve(max_iterations=20000, tolerance=1e-9,
+                     preconditioner=cg.PRECOND_LEARNED, precision=cg.PRECISION_MIXED)
+        r["untrained_learned_mixed"] = {"ms": ri["solve_ms"], "iterations": ri["iterations"]}
+        res.append(r)
+    summary = summarize(res)
+    meta = {"seed": a.seed, "steps": steps, "train_seconds": train_s,
+            "selected_epoch": selected, "generate_seconds": gen_s,
+            "config": {"family": "geometric graph", "points": a.points, "mean_degree": 12,
+                       "weights": "exp(-d/r)", "shift": 1e-3, "train": a.train,
+                       "heldout": a.heldout, "epochs": a.epochs, "lr": a.lr, "eps": a.eps,
+                       "probes": 8, "smooth_steps": a.smooth_steps,
+                       "smooth_cols": a.smooth_cols, "smooth_scale": a.smooth_scale,
+                       "select": a.select, "residual_probes": a.residual_probes,
                        "residual_its": res_its,
                        "loss": "||(Ghat^T Ahat Ghat - I) V||^2 / (N S), Rademacher V"},
             "log": log, "heldout": summary}
