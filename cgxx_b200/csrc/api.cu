@@ -144,6 +144,7 @@ struct cgx_handle {
   int *ptr = nullptr, *index = nullptr;  // CRS
   double *value = nullptr;
   int tile_cap = 0;
+  int warp_cap = 0;  // k_crs_warp's tile capacity when 256-row tiles overflow
   int *ell_length = nullptr, *ell_index = nullptr;  // ELL
   double *ell_data = nullptr;
   int ell_width = 0;
@@ -357,6 +358,23 @@ __global__ void k_loop_guard(CgState *st) {
 template <typename VT, typename IT, typename Op>
 static cudaError_t launch_crs_view(cgx_handle *h, CrsView<VT, IT> A,
                                    const typename Comp<VT>::T *x, Op op) {
+  if (A.warp_cap > 0) {
+    const size_t smem = 16 * kWarps + kWarps * crs_stage_bytes<VT, IT>(A.warp_cap);
+    auto kern = k_crs_warp<VT, IT, Op>;
+    cudaError_t e;
+    if (smem > 48 * 1024 &&
+        (e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)smem)) != cudaSuccess)
+      return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem);
+    if (e != cudaSuccess) return e;
+    const int wtiles = (h->N + 31) / 32;
+    const int grid = std::max(1, std::min(std::min(h->num_sms * std::max(1, per_sm), kMaxGrid),
+                                          (wtiles + kWarps - 1) / kWarps));
+    kern<<<grid, kThreads, smem, h->stream>>>(A, x, op, h->st, h->partials);
+    return cudaGetLastError();
+  }
   const int cap = A.tile_cap;
   const size_t smem = crs_smem_bytes<VT, IT>(cap);
   auto kern = k_crs<VT, IT, Op>;
@@ -381,7 +399,7 @@ template <typename VT, typename Op>
 static cudaError_t launch_crs(cgx_handle *h, const VT *value, int cap,
                               const VT *x, Op op) {
   return launch_crs_view<VT, int, Op>(
-      h, CrsView<VT, int>{h->ptr, h->index, value, h->N, cap}, x, op);
+      h, CrsView<VT, int>{h->ptr, h->index, value, h->N, cap, h->warp_cap}, x, op);
 }
 
 template <typename Op>
@@ -487,10 +505,12 @@ static cudaError_t launch_inner_q(cgx_handle *h) {
     return launch_sellu(h, h->sa, h->sa_val, h->p32, op);
   if (h->compact16)
     return launch_crs_view(
-        h, CrsView<float, int16_t>{h->ptr, h->idx16, h->value32, h->N, h->tile_cap},
+        h, CrsView<float, int16_t>{h->ptr, h->idx16, h->value32, h->N, h->tile_cap,
+                                   h->warp_cap},
         h->p32, op);
   return launch_crs_view(
-      h, CrsView<float, int>{h->ptr, h->index, h->value32, h->N, h->tile_cap},
+      h, CrsView<float, int>{h->ptr, h->index, h->value32, h->N, h->tile_cap,
+                             h->warp_cap},
       h->p32, op);
 }
 
@@ -869,6 +889,15 @@ cgx_status cgx_upload_crs(cgx_handle *h, int N, int nz, const int *ptr,
     maxTile = std::max(maxTile, ptr[r1] - ptr[r0]);
   }
   h->tile_cap = std::min(maxTile, 4096);
+  // Rows too long for those tiles: 32-row tiles staged per warp (k_crs_warp)
+  // when they hold at most 2048 nonzeros.
+  h->warp_cap = 0;
+  if (maxTile > 4096) {
+    int maxWarp = 0;
+    for (int r0 = 0; r0 < N; r0 += 32)
+      maxWarp = std::max(maxWarp, ptr[std::min(N, r0 + 32)] - ptr[r0]);
+    if (maxWarp <= 2048) h->warp_cap = maxWarp;
+  }
 
   Carver c;
   size_t o_ptr = c.take<int>((size_t)N + 1 + kPad);

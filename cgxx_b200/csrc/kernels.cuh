@@ -32,6 +32,8 @@ struct CrsView {
   const VT *value;
   int N;
   int tile_cap;  // max nonzeros of a staged 256-row tile; 0 disables staging
+  int warp_cap;  // > 0: 256-row tiles overflow tile_cap, and k_crs_warp stages
+                 // 32-row tiles of up to warp_cap nonzeros instead
 };
 
 // Arithmetic type of a value storage type: half values are widened to FP32.
@@ -242,6 +244,80 @@ __global__ void __launch_bounds__(kThreads)
       op.row(row, sum, acc);
     }
     __syncthreads();
+  }
+  op.finish(acc, st, partials);
+}
+
+// CRS SpMV for rows too long for k_crs's 256-row tiles (a tile above its
+// capacity would take the direct path, whose per-thread row loads do not
+// coalesce): each warp stages its own 32-row tiles (warp w of the grid takes
+// tiles w, w + warps, ...). One lane issues the tile's two 1-D bulk copies
+// into the warp's shared-memory slot (A.warp_cap nonzeros) on the warp's
+// mbarrier, and every lane then sums its row from the slot in storage order,
+// as k_crs does, so the FP64 result is the same. One stage per warp: the
+// copies of the SM's other warps overlap a warp's summation.
+template <typename VT, typename IT, typename Op,
+          typename XT = typename Comp<VT>::T>
+__global__ void __launch_bounds__(kThreads)
+    k_crs_warp(CrsView<VT, IT> A, const XT *__restrict__ x, Op op, CgState *st,
+               double *partials) {
+  if (op.skip(st)) return;
+  extern __shared__ __align__(16) unsigned char smem[];
+  constexpr int VPER = vals_per_16B<VT>();
+  constexpr int IPER = vals_per_16B<IT>();
+  const int cap = A.warp_cap;
+  const int N = A.N;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
+  const size_t vbytes = align16((size_t)(cap + 16) * sizeof(VT));
+  const size_t sbytes = crs_stage_bytes<VT, IT>(cap);
+  unsigned char *slot = smem + 16 * kWarps + (size_t)warp * sbytes;
+  VT *sv = reinterpret_cast<VT *>(slot);
+  IT *si = reinterpret_cast<IT *>(slot + vbytes);
+  if (threadIdx.x == 0) {
+    for (int w = 0; w < kWarps; w++) mbar_init(&bars[w], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+
+  typename Op::Acc acc;
+  unsigned phase = 0;
+  const int ntiles = (N + 31) >> 5;
+  const int nw = gridDim.x * kWarps;
+  for (int t = blockIdx.x * kWarps + warp; t < ntiles; t += nw) {
+    const int r0 = t << 5, r1 = min(N, r0 + 32);
+    const int s = __ldg(&A.ptr[r0]), e = __ldg(&A.ptr[r1]);
+    const bool staged = e > s && e - s <= cap;
+    const int row = r0 + lane;
+    const int j0 = row < r1 ? __ldg(&A.ptr[row]) : 0;
+    const int j1 = row < r1 ? __ldg(&A.ptr[row + 1]) : 0;
+    const int vs = s & ~(VPER - 1), is = s & ~(IPER - 1);
+    bool ok = true;
+    if (staged) {
+      if (lane == 0) {
+        const int ve = (e + VPER - 1) & ~(VPER - 1);
+        const int ie = (e + IPER - 1) & ~(IPER - 1);
+        const unsigned vb = (unsigned)(ve - vs) * (unsigned)sizeof(VT);
+        const unsigned ib = (unsigned)(ie - is) * (unsigned)sizeof(IT);
+        mbar_arrive_expect_tx(&bars[warp], vb + ib);
+        bulk_g2s(sv, A.value + vs, vb, &bars[warp]);
+        bulk_g2s(si, A.index + is, ib, &bars[warp]);
+      }
+      ok = mbar_wait_bounded(&bars[warp], phase);
+      phase ^= 1u;
+      if (!ok && lane == 0) atomicOr(&st->error, kErrBarrierTimeout);
+    }
+    if (row < r1) {
+      XT sum = 0;
+      if (staged) {
+        if (ok) sum = row_sum_staged<VT, IT, 8>(row, j0, j1, sv - vs, si - is, x);
+      } else {
+        for (int j = j0; j < j1; j++)
+          sum = madd(sum, A.value[j], __ldg(&x[column(row, A.index[j])]));
+      }
+      op.row(row, sum, acc);
+    }
+    __syncwarp();  // the slot is read before the warp's next copy lands
   }
   op.finish(acc, st, partials);
 }
