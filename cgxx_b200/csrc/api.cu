@@ -1351,6 +1351,11 @@ static cgx_status ensure_f32(cgx_handle *h) {
   if (!h->sa_tried) {
     h->sa_tried = true;
     CGX_TRY(build_sellu(h, h->ptr, h->index, (size_t)h->nz, h->sa));
+    // Mostly per-row slices (an irregular matrix) pad every row of a slice
+    // to its longest one; A's FP32 CRS is faster there (measured on the 2M
+    // point geometric graph: 64 against 71 us per product).
+    if (h->sa.ok && 2 * h->sa.uniform < (long long)((h->N + 31) / 32))
+      sellu_free(h->sa);
   }
   if (h->sa.ok && !h->sa_val) {
     CUDA_TRY(cudaMalloc(&h->sa_val, sizeof(float) * (h->sa.slots + kPad)));

@@ -161,10 +161,11 @@ def _shuffle_rows(A, seed):
 
 @pytest.mark.parametrize("case", ["ragged", "unsorted", "wide", "stencil27_odd"])
 def test_mixed_on_irregular_patterns(handle, case):
-    """The FP32 inner SpMV's sliced layout: uniform slices (stencils, with
-    zero-filled missing neighbours at the boundary), per-row slices (ragged
-    random rows, rows whose offsets span more than 32 slots, unsorted rows)
-    and a last slice shorter than 32 rows (N not a multiple of 32)."""
+    """The FP32 inner SpMV on both of its forms: the SELL-U layout for a
+    stencil (uniform slices with zero-filled missing neighbours at the
+    boundary, a last slice shorter than 32 rows) and FP32 CRS for matrices
+    whose slices would be mostly per-row (ragged random rows, rows whose
+    offsets span more than 32 slots, unsorted rows)."""
     if case == "ragged":
         A = random_crs(1007, max_len=12, seed=3, spd=True)
     elif case == "unsorted":
@@ -186,12 +187,13 @@ def test_mixed_on_irregular_patterns(handle, case):
     assert tr <= 1e-9
     _, it_o, outer_o, _ = O.mixed_ir_solve(A.ptr, A.index, A.value, Cd, b)
     assert abs(res["iterations"] - it_o) <= 0.05 * it_o + 2
+    # A stencil keeps the SELL-U layout (every slice uniform); matrices whose
+    # slices are mostly per-row run the inner SpMV on FP32 CRS.
     slots, uniform, slices = handle.inner_layout()
-    assert slices == (A.N + 31) // 32 and slots >= A.nz
     if case == "stencil27_odd":
-        assert uniform == slices
-    elif case == "unsorted":
-        assert uniform == 0
+        assert slices == (A.N + 31) // 32 and uniform == slices and slots >= A.nz
+    else:
+        assert slots == 0
 
 
 def test_time_spmv_measures_the_fused_product(handle):
