@@ -141,15 +141,13 @@ struct cgx_handle {
   int N = 0;
   int nz = 0;
   void *mat_mem = nullptr;
-  int *ptr = nullptr, *index = nullptr;  // CRS
+  int *ptr = nullptr, *index = nullptr;  // CRS, and COO grouped by row
   double *value = nullptr;
   int tile_cap = 0;
   int warp_cap = 0;  // k_crs_warp's tile capacity when 256-row tiles overflow
   int *ell_length = nullptr, *ell_index = nullptr;  // ELL
   double *ell_data = nullptr;
   int ell_width = 0;
-  int *coo_start = nullptr, *coo_perm = nullptr, *coo_J = nullptr;  // COO
-  double *coo_V = nullptr;
 
   // Vectors K X P Q R Z and Jacobi C.
   void *vec_mem = nullptr;
@@ -276,8 +274,6 @@ static void free_matrix(cgx_handle *h) {
   h->value = nullptr;
   h->ell_length = h->ell_index = nullptr;
   h->ell_data = nullptr;
-  h->coo_start = h->coo_perm = h->coo_J = nullptr;
-  h->coo_V = nullptr;
   for (auto &v : h->vec) v = nullptr;
   h->C = nullptr;
   h->tmp = nullptr;
@@ -314,6 +310,20 @@ __global__ void k_validate_crs(int N, int nz, const int *ptr, const int *index,
   }
 }
 
+// Column-major (element (i, j) at j * N + i) to the tile-major device layout.
+__global__ void k_ell_tiles(int N, int width, const int *__restrict__ ci,
+                            const double *__restrict__ cd, int *__restrict__ ti,
+                            double *__restrict__ td) {
+  const size_t total = (size_t)N * (size_t)width;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (size_t)gridDim.x * blockDim.x) {
+    const int j = (int)(e / (size_t)N), i = (int)(e - (size_t)j * N);
+    const size_t o = ell_at(i, j, width);
+    ti[o] = ci[e];
+    td[o] = cd[e];
+  }
+}
+
 __global__ void k_validate_ell(int N, int width, const int *length,
                                const int *index, int *flag) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N;
@@ -324,17 +334,9 @@ __global__ void k_validate_ell(int N, int width, const int *length,
       continue;
     }
     for (int j = 0; j < len; j++) {
-      int c = index[(size_t)j * N + i];
+      int c = index[ell_at(i, j, width)];
       if (c < 0 || c >= N) atomicOr(flag, 2);
     }
-  }
-}
-
-__global__ void k_validate_coo(int N, int nz, const int *J, int *flag) {
-  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nz;
-       j += gridDim.x * blockDim.x) {
-    int c = J[j];
-    if (c < 0 || c >= N) atomicOr(flag, 2);
   }
 }
 
@@ -406,18 +408,30 @@ template <typename Op>
 static cudaError_t launch_spmv(cgx_handle *h, const double *x, Op op) {
   switch (h->format) {
   case CGX_FORMAT_CRS:
+  case CGX_FORMAT_COO:  // held in the row-grouped layout (cgx_upload_coo)
     return launch_crs<double, Op>(h, h->value, h->tile_cap, x, op);
   case CGX_FORMAT_ELL: {
     EllView<double> A{h->ell_length, h->ell_index, h->ell_data, h->N,
                       h->ell_width};
-    k_ell<double, Op><<<grid_stream(h, h->N), kThreads, 0, h->stream>>>(
-        A, x, op, h->st, h->partials);
-    return cudaGetLastError();
-  }
-  case CGX_FORMAT_COO: {
-    CooView A{h->coo_start, h->coo_perm, h->coo_J, h->coo_V, h->N};
-    k_coo<Op><<<grid_stream(h, h->N), kThreads, 0, h->stream>>>(
-        A, x, op, h->st, h->partials);
+    if (h->ell_width >= 1 && h->ell_width <= kEllStagedWidth) {
+      const size_t smem = ell_smem_bytes<double>(h->ell_width);
+      auto kern = k_ell_tma<double, Op>;
+      cudaError_t e;
+      if (smem > 48 * 1024 &&
+          (e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem)) != cudaSuccess)
+        return e;
+      int per_sm = 0;
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem);
+      if (e != cudaSuccess) return e;
+      const int tiles = (h->N + kThreads - 1) / kThreads;
+      const int grid = std::max(1, std::min(std::min(h->num_sms * std::max(1, per_sm),
+                                                     kMaxGrid), tiles));
+      kern<<<grid, kThreads, smem, h->stream>>>(A, x, op, h->st, h->partials);
+    } else {
+      k_ell<double, Op><<<grid_stream(h, h->N), kThreads, 0, h->stream>>>(
+          A, x, op, h->st, h->partials);
+    }
     return cudaGetLastError();
   }
   }
@@ -869,14 +883,11 @@ static cgx_status check_flag(cgx_handle *h, const char *what) {
 
 extern "C" {
 
-cgx_status cgx_upload_crs(cgx_handle *h, int N, int nz, const int *ptr,
-                          const int *index, const double *value) {
-  if (!h) return fail(CGX_ERROR_INVALID_ARGUMENT, "handle is NULL");
-  if (N <= 0 || nz < 0 || !ptr || (nz > 0 && (!index || !value)))
-    return fail(CGX_ERROR_INVALID_ARGUMENT, "bad CRS sizes or pointers");
-  if (ptr[0] != 0 || ptr[N] != nz)
-    return fail(CGX_ERROR_INVALID_ARGUMENT,
-                "CRS ptr must start at 0 and end at nz");
+// Row-grouped device layout shared by CRS and COO: row pointers, column
+// indices and values in storage order, validated on the device.
+static cgx_status upload_rows(cgx_handle *h, int N, int nz, const int *ptr,
+                              const int *index, const double *value,
+                              int format, const char *what) {
   DeviceGuard guard(h->device);
   CUDA_TRY(cudaStreamSynchronize(h->stream));
   free_matrix(h);
@@ -919,13 +930,24 @@ cgx_status cgx_upload_crs(cgx_handle *h, int N, int nz, const int *ptr,
   }
   h->N = N;
   h->nz = nz;
-  h->format = CGX_FORMAT_CRS;
+  h->format = format;
   CGX_TRY(alloc_vectors(h, N));
   CUDA_TRY(cudaMemsetAsync(h->flag, 0, sizeof(int), h->stream));
   k_validate_crs<<<grid_stream(h, std::max(N, nz)), kThreads, 0, h->stream>>>(
       N, nz, h->ptr, h->index, h->flag);
   CUDA_TRY(cudaGetLastError());
-  return check_flag(h, "CRS");
+  return check_flag(h, what);
+}
+
+cgx_status cgx_upload_crs(cgx_handle *h, int N, int nz, const int *ptr,
+                          const int *index, const double *value) {
+  if (!h) return fail(CGX_ERROR_INVALID_ARGUMENT, "handle is NULL");
+  if (N <= 0 || nz < 0 || !ptr || (nz > 0 && (!index || !value)))
+    return fail(CGX_ERROR_INVALID_ARGUMENT, "bad CRS sizes or pointers");
+  if (ptr[0] != 0 || ptr[N] != nz)
+    return fail(CGX_ERROR_INVALID_ARGUMENT,
+                "CRS ptr must start at 0 and end at nz");
+  return upload_rows(h, N, nz, ptr, index, value, CGX_FORMAT_CRS, "CRS");
 }
 
 cgx_status cgx_upload_ell(cgx_handle *h, int N, int nz, int maxNz,
@@ -938,7 +960,10 @@ cgx_status cgx_upload_ell(cgx_handle *h, int N, int nz, int maxNz,
   DeviceGuard guard(h->device);
   CUDA_TRY(cudaStreamSynchronize(h->stream));
   free_matrix(h);
-  const size_t elems = (size_t)maxNz * (size_t)N;
+  // The caller's column-major arrays go through a temporary device copy into
+  // the tile-major layout (ell_at).
+  const size_t elems = ell_elems(N, maxNz);
+  const size_t celems = (size_t)maxNz * (size_t)N;
   Carver c;
   size_t o_len = c.take<int>((size_t)N + kPad);
   size_t o_idx = c.take<int>(elems + kPad);
@@ -952,11 +977,26 @@ cgx_status cgx_upload_ell(cgx_handle *h, int N, int nz, int maxNz,
   CUDA_TRY(cudaMemsetAsync(h->mat_mem, 0, c.off, h->stream));
   CUDA_TRY(cudaMemcpyAsync(h->ell_length, length, sizeof(int) * (size_t)N,
                            cudaMemcpyHostToDevice, h->stream));
-  if (elems > 0) {
-    CUDA_TRY(cudaMemcpyAsync(h->ell_index, index, sizeof(int) * elems,
-                             cudaMemcpyHostToDevice, h->stream));
-    CUDA_TRY(cudaMemcpyAsync(h->ell_data, data, sizeof(double) * elems,
-                             cudaMemcpyHostToDevice, h->stream));
+  if (celems > 0) {
+    void *tmp = nullptr;
+    Carver t;
+    const size_t o_ti = t.take<int>(celems), o_td = t.take<double>(celems);
+    CUDA_TRY(cudaMalloc(&tmp, t.off));
+    int *ci = (int *)((char *)tmp + o_ti);
+    double *cd = (double *)((char *)tmp + o_td);
+    cudaError_t e = cudaMemcpyAsync(ci, index, sizeof(int) * celems,
+                                    cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(cd, data, sizeof(double) * celems,
+                          cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) {
+      k_ell_tiles<<<grid_stream(h, celems), kThreads, 0, h->stream>>>(
+          N, maxNz, ci, cd, h->ell_index, h->ell_data);
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    cudaFree(tmp);
+    CUDA_TRY(e);
   }
   h->N = N;
   h->nz = nz;
@@ -974,9 +1014,13 @@ cgx_status cgx_upload_coo(cgx_handle *h, int N, int nz, const int *I,
   if (!h) return fail(CGX_ERROR_INVALID_ARGUMENT, "handle is NULL");
   if (N <= 0 || nz < 0 || (nz > 0 && (!I || !J || !V)))
     return fail(CGX_ERROR_INVALID_ARGUMENT, "bad COO sizes or pointers");
-  // Row-grouped permutation in entry order (stable counting sort on the
-  // host): keeps serial/SerialCG.cpp:79-85's per-row summation order.
-  std::vector<int> start((size_t)N + 1, 0), perm((size_t)(nz > 0 ? nz : 1));
+  // serial/SerialCG.cpp:79-85 computes y = 0, then y[I[e]] += V[e] * x[J[e]]
+  // for e in entry order, so each row's sum runs over its entries in entry
+  // order. A stable counting sort by row on the host groups the entries that
+  // way; the device then holds the row-grouped layout and runs the CRS SpMV,
+  // which sums each row in storage order: the same products, the same order,
+  // no atomics.
+  std::vector<int> start((size_t)N + 1, 0);
   for (int e = 0; e < nz; e++) {
     if (I[e] < 0 || I[e] >= N)
       return fail(CGX_ERROR_INVALID_ARGUMENT,
@@ -984,46 +1028,20 @@ cgx_status cgx_upload_coo(cgx_handle *h, int N, int nz, const int *I,
     start[(size_t)I[e] + 1]++;
   }
   for (int i = 0; i < N; i++) start[i + 1] += start[i];
+  std::vector<int> Jr((size_t)(nz > 0 ? nz : 1));
+  std::vector<double> Vr((size_t)(nz > 0 ? nz : 1));
   {
     std::vector<int> fill(start.begin(), start.end() - 1);
-    for (int e = 0; e < nz; e++) perm[fill[I[e]]++] = e;
+    for (int e = 0; e < nz; e++) {
+      const int k = fill[I[e]]++;
+      Jr[k] = J[e];
+      Vr[k] = V[e];
+    }
   }
-  DeviceGuard guard(h->device);
-  CUDA_TRY(cudaStreamSynchronize(h->stream));
-  free_matrix(h);
-  Carver c;
-  size_t o_st = c.take<int>((size_t)N + 1 + kPad);
-  size_t o_pm = c.take<int>((size_t)nz + kPad);
-  size_t o_j = c.take<int>((size_t)nz + kPad);
-  size_t o_v = c.take<double>((size_t)nz + kPad);
-  CUDA_TRY(cudaMalloc(&h->mat_mem, c.off));
-  char *base = (char *)h->mat_mem;
-  h->coo_start = (int *)(base + o_st);
-  h->coo_perm = (int *)(base + o_pm);
-  h->coo_J = (int *)(base + o_j);
-  h->coo_V = (double *)(base + o_v);
-  CUDA_TRY(cudaMemcpyAsync(h->coo_start, start.data(),
-                           sizeof(int) * ((size_t)N + 1),
-                           cudaMemcpyHostToDevice, h->stream));
-  if (nz > 0) {
-    CUDA_TRY(cudaMemcpyAsync(h->coo_perm, perm.data(), sizeof(int) * nz,
-                             cudaMemcpyHostToDevice, h->stream));
-    CUDA_TRY(cudaMemcpyAsync(h->coo_J, J, sizeof(int) * nz,
-                             cudaMemcpyHostToDevice, h->stream));
-    CUDA_TRY(cudaMemcpyAsync(h->coo_V, V, sizeof(double) * nz,
-                             cudaMemcpyHostToDevice, h->stream));
-  }
-  h->N = N;
-  h->nz = nz;
-  h->format = CGX_FORMAT_COO;
-  CGX_TRY(alloc_vectors(h, N));
-  CUDA_TRY(cudaMemsetAsync(h->flag, 0, sizeof(int), h->stream));
-  k_validate_coo<<<grid_stream(h, nz), kThreads, 0, h->stream>>>(
-      N, nz, h->coo_J, h->flag);
-  CUDA_TRY(cudaGetLastError());
-  // The host vectors above must outlive the asynchronous copies.
-  CUDA_TRY(cudaStreamSynchronize(h->stream));
-  return check_flag(h, "COO");
+  // upload_rows returns after a stream synchronisation, so the host vectors
+  // outlive the copies.
+  return upload_rows(h, N, nz, start.data(), Jr.data(), Vr.data(),
+                     CGX_FORMAT_COO, "COO");
 }
 
 static cgx_status need_matrix(cgx_handle *h) {

@@ -55,6 +55,13 @@ __device__ __forceinline__ int column(int row, int16_t stored) {
   return row + (int)stored;
 }
 
+// ELL on the device, tile-major: rows are cut into 256-row tiles and tile t
+// holds its slots one after another, each as 256 consecutive entries, so
+// element (i, j) is at (t * width + j) * 256 + i % 256 with t = i / 256. The
+// reference's column-major array (element (i, j) at j * N + i) is rearranged
+// this way at upload. Within a slot, consecutive rows are adjacent, as in the
+// column-major form, and a whole tile is one contiguous block. The last tile
+// is allocated in full (its gap rows are zero).
 template <typename VT>
 struct EllView {
   const int *length;
@@ -63,6 +70,14 @@ struct EllView {
   int N;
   int width;
 };
+
+static_assert(kThreads == 256, "ELL tiles are the 256-row CTA tiles");
+__host__ __device__ inline size_t ell_at(int i, int j, int width) {
+  return ((size_t)(i >> 8) * (size_t)width + (size_t)j) * 256 + (size_t)(i & 255);
+}
+__host__ __device__ inline size_t ell_elems(int N, int width) {
+  return (((size_t)N + 255) >> 8) * 256 * (size_t)width;
+}
 
 // Multiply-add of one matrix entry. FP64 keeps the reference's separate
 // rounding; FP32 (the inner solve of the mixed path) uses an FMA.
@@ -341,11 +356,98 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 // ---------------------------------------------------------------------------
-// ELL SpMV: column-major storage, element (i, j) at j*N + i with 64-bit
-// offsets; consecutive threads read consecutive rows, so every load of a
-// column is coalesced. Rows stop at length[i] (the reference leaves padding
-// slots uninitialised, Matrix.cpp:339-361).
+// ELL SpMV. Rows stop at length[i] (the reference leaves padding slots
+// uninitialised, Matrix.cpp:339-361), and each row is summed from 0 over its
+// slots in order, so the FP64 result equals the reference's.
+//
+// k_ell_tma, persistent, for widths up to kEllStagedWidth: CTA b handles
+// 256-row tiles b, b + grid, ... One thread brings a tile's values and
+// indices (two contiguous blocks of the tile-major layout) into shared memory
+// with two 1-D bulk copies (TMA) one tile ahead, double-buffered on two
+// mbarriers, as k_crs does for a CRS tile. The x gathers go through the
+// read-only path and mostly hit L2.
 
+constexpr int kEllStagedWidth = 16;
+
+template <typename VT>
+__host__ __device__ inline size_t ell_stage_bytes(int width) {
+  return (size_t)width * kThreads * (sizeof(VT) + sizeof(int));
+}
+template <typename VT>
+__host__ __device__ inline size_t ell_smem_bytes(int width) {
+  return 16 + 2 * ell_stage_bytes<VT>(width);
+}
+
+template <typename VT, typename Op>
+__global__ void __launch_bounds__(kThreads)
+    k_ell_tma(EllView<VT> A, const VT *__restrict__ x, Op op, CgState *st,
+              double *partials) {
+  if (op.skip(st)) return;
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int W = A.width, N = A.N;
+  const int nTiles = (N + kThreads - 1) / kThreads;
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
+  const size_t sbytes = ell_stage_bytes<VT>(W);
+  const size_t vbytes = (size_t)W * kThreads * sizeof(VT);
+  if (threadIdx.x == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+
+  // A tile is two contiguous blocks (values, indices) of the tile-major
+  // layout: one bulk copy each.
+  auto issue = [&](int t, int buf) {
+    unsigned char *stage = smem + 16 + (size_t)buf * sbytes;
+    const size_t base = (size_t)t * W * kThreads;
+    mbar_arrive_expect_tx(&bars[buf], (unsigned)sbytes);
+    bulk_g2s(stage, A.data + base, (unsigned)vbytes, &bars[buf]);
+    bulk_g2s(stage + vbytes, A.index + base, (unsigned)(sbytes - vbytes),
+             &bars[buf]);
+  };
+
+  typename Op::Acc acc;
+  unsigned ph0 = 0, ph1 = 0;
+  int k = 0;
+  int t = blockIdx.x;
+  if (threadIdx.x == 0 && t < nTiles) issue(t, 0);
+  for (; t < nTiles; t += gridDim.x, k++) {
+    const int buf = k & 1;
+    const int tn = t + gridDim.x;
+    if (threadIdx.x == 0 && tn < nTiles) issue(tn, buf ^ 1);
+    const int row = t * kThreads + threadIdx.x;
+    const int len = row < N ? __ldg(&A.length[row]) : 0;
+    const bool ok = mbar_wait_bounded(&bars[buf], buf ? ph1 : ph0);
+    if (buf) ph1 ^= 1u; else ph0 ^= 1u;
+    if (!ok && threadIdx.x == 0) atomicOr(&st->error, kErrBarrierTimeout);
+    if (row < N) {
+      VT sum = 0;
+      if (ok) {
+        const unsigned char *stage = smem + 16 + (size_t)buf * sbytes;
+        const VT *sv = reinterpret_cast<const VT *>(stage) + threadIdx.x;
+        const int *si =
+            reinterpret_cast<const int *>(stage + vbytes) + threadIdx.x;
+        for (int j0 = 0; j0 < len; j0 += 8) {
+          VT xv[8];
+#pragma unroll
+          for (int u = 0; u < 8; u++)
+            if (j0 + u < len) xv[u] = __ldg(&x[si[(j0 + u) * kThreads]]);
+#pragma unroll
+          for (int u = 0; u < 8; u++)
+            if (j0 + u < len) sum = madd(sum, sv[(j0 + u) * kThreads], xv[u]);
+        }
+      }
+      op.row(row, sum, acc);
+    }
+    __syncthreads();
+  }
+  op.finish(acc, st, partials);
+}
+
+// k_ell, for wider rows: one thread per row, loads straight from global
+// memory; consecutive threads read consecutive rows, so every load of a
+// column is coalesced.
 template <typename VT, typename Op>
 __global__ void __launch_bounds__(kThreads)
     k_ell(EllView<VT> A, const VT *__restrict__ x, Op op, CgState *st,
@@ -356,46 +458,12 @@ __global__ void __launch_bounds__(kThreads)
   for (int row = blockIdx.x * kThreads + threadIdx.x; row < N;
        row += gridDim.x * kThreads) {
     const int len = __ldg(&A.length[row]);
-    const VT *dat = A.data + row;
-    const int *idx = A.index + row;
-    const size_t n = (size_t)N;
+    const size_t o = ell_at(row, 0, A.width);
+    const VT *dat = A.data + o;
+    const int *idx = A.index + o;
     const VT sum = row_sum<VT, 4>(
-        0, len, [&](int j) { return __ldg(&dat[(size_t)j * n]); },
-        [&](int j) { return __ldg(&idx[(size_t)j * n]); }, x);
-    op.row(row, sum, acc);
-  }
-  op.finish(acc, st, partials);
-}
-
-// ---------------------------------------------------------------------------
-// COO SpMV (serial/SerialCG.cpp:79-85 computes y = 0, then y[I] += V*x[J] in
-// entry order). Entries of one row are contiguous in the file order the
-// reference produces for sorted inputs but not in general, so the device
-// version sums each row's entries in entry order through a row-sorted
-// permutation built at upload time: perm lists the entry ids of row i, in
-// entry order, at [rowStart[i], rowStart[i+1]). That keeps the reference's
-// summation order and makes the product deterministic without atomics.
-
-struct CooView {
-  const int *rowStart;  // N+1
-  const int *perm;      // nz entry ids, grouped by row, entry order
-  const int *J;
-  const double *V;
-  int N;
-};
-
-template <typename Op>
-__global__ void __launch_bounds__(kThreads)
-    k_coo(CooView A, const double *__restrict__ x, Op op, CgState *st,
-          double *partials) {
-  if (op.skip(st)) return;
-  typename Op::Acc acc;
-  for (int row = blockIdx.x * kThreads + threadIdx.x; row < A.N;
-       row += gridDim.x * kThreads) {
-    const int j0 = __ldg(&A.rowStart[row]), j1 = __ldg(&A.rowStart[row + 1]);
-    const double sum = row_sum<double>(
-        j0, j1, [&](int j) { return __ldg(&A.V[__ldg(&A.perm[j])]); },
-        [&](int j) { return __ldg(&A.J[__ldg(&A.perm[j])]); }, x);
+        0, len, [&](int j) { return __ldg(&dat[j * kThreads]); },
+        [&](int j) { return __ldg(&idx[j * kThreads]); }, x);
     op.row(row, sum, acc);
   }
   op.finish(acc, st, partials);

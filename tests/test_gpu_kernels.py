@@ -62,6 +62,30 @@ def test_spmv_ell_bitexact(handle, N):
     assert np.array_equal(handle.get_vector("Q"), O.matvec_ell(N, length, index, data, x))
 
 
+@pytest.mark.parametrize("width", [1, 7, 16])
+@pytest.mark.parametrize("N", SIZES)
+def test_spmv_ell_staged_bitexact(handle, N, width):
+    # Widths up to 16 take the bulk-copy staged kernel. The reference leaves
+    # padding slots uninitialised (Matrix.cpp:339-361): they hold NaN values
+    # and out-of-range indices here, which must never be read. Empty rows and
+    # sizes that are not a multiple of the 256-row tile are included.
+    from cgxx_b200 import generators as G
+    A = random_crs(N, 0, width, seed=N + width)
+    max_nz, length, index, data = G.to_ell(A)
+    assert max_nz <= width
+    slot = np.arange(max_nz)[:, None]
+    pad = (slot >= length[None, :]).reshape(-1)
+    index = index.copy()
+    data = data.copy()
+    index[pad] = -(N + 3)
+    data[pad] = np.nan
+    handle.upload_ell(N, A.nz, max_nz, length, index, data)
+    x = _x(N, 3)
+    handle.set_vector("X", x)
+    handle.matvec("X", "Q")
+    assert np.array_equal(handle.get_vector("Q"), O.matvec_ell(N, length, index, data, x))
+
+
 @pytest.mark.parametrize("N", SIZES)
 def test_spmv_coo_bitexact(handle, N):
     rng = np.random.default_rng(N)
