@@ -1,7 +1,8 @@
 // Device kernels of libcgb200.
 //
-// Sparse matrix-vector products (CRS with bulk-copy staging, column-major
-// ELL, COO), each taking a row epilogue ("Op") so that the product is fused
+// Sparse matrix-vector products (CRS and tile-major ELL, both staged by
+// bulk copies; COO runs on its row-grouped CRS), each taking a row epilogue
+// ("Op") so that the product is fused
 // with whatever the conjugate-gradient step does with the row result: store
 // it, form a dot product, form the residual, ... Ops with accumulators end
 // with a deterministic grid-wide reduction whose last CTA runs the Op's
