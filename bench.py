@@ -475,7 +475,17 @@ def our_arm(args, world, rank, local):
     else:
         kk = kern[args.path]
         slots, uniform, slices = h.inner_layout()
-        if slots:
+        band = h.inner_band()
+        prof_name = "spmv_sellu_fp32_diffusion7_160.json"
+        if band:
+            # Symmetric band: 4 FP32 values per row (diagonal and upper half;
+            # the lower half is read from the rows above, in L1/L2), p once,
+            # q written.
+            fp32_spmv_bytes = 16 * N + 8 * N
+            kname = (f"k_band<4, OpInnerQ>: q = A p fused with <p,q> (FP32 symmetric band, "
+                     f"offsets {band})")
+            prof_name = "spmv_band_fp32_diffusion7_160.json"
+        elif slots:
             # SELL-U: FP32 values, 16-byte slice descriptors, p once, q
             # written (a uniform slice carries no per-entry index).
             fp32_spmv_bytes = 4 * nnz + 16 * slices + 8 * N
@@ -488,7 +498,7 @@ def our_arm(args, world, rank, local):
                 "peak": peak, "unit": "GB/s", "kernel": kname,
                 "algorithmic_bytes": fp32_spmv_bytes, "peak_kind": peak_kind}
         roof["frac"] = roof["achieved"] / peak
-        prof32 = read_traffic_profile("spmv_sellu_fp32_diffusion7_160.json", args)
+        prof32 = read_traffic_profile(prof_name, args)
         roof["traffic"] = prof32.get("dram_bytes_per_launch") if prof32 else None
 
     # End to end through the public C ABI: pinned host inputs uploaded every

@@ -105,6 +105,8 @@ PROTOTYPES = {
     "cgx_time_spmv": [_P, _I, _I, _PD],
     "cgx_inner_layout": [_P, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),
                          C.POINTER(C.c_longlong)],
+    "cgx_inner_band": [_P, _PI, _PI],
+    "cgx_inner_matvec": [_P, _P, _P],
     "cgx_mtx_read": [C.c_char_p, _PI, _PI, C.POINTER(_PI), C.POINTER(_PI),
                      C.POINTER(_PD)],
     "cgx_mtx_write_symmetric_crs": [C.c_char_p, _I, _P, _P, _P],
@@ -302,6 +304,21 @@ class Handle:
         a, b, c = C.c_longlong(), C.c_longlong(), C.c_longlong()
         check(self._lib.cgx_inner_layout(self._h, C.byref(a), C.byref(b), C.byref(c)))
         return a.value, b.value, c.value
+
+    def inner_band(self):
+        """Offsets (ascending from 0) stored per row by the symmetric band
+        form of A's FP32 copy; empty when the inner SpMV uses another form."""
+        k = C.c_int()
+        offs = (C.c_int * 4)()
+        check(self._lib.cgx_inner_band(self._h, C.byref(k), offs))
+        return [offs[i] for i in range(k.value)]
+
+    def inner_matvec(self, x):
+        """y = A x (float32) by the inner FP32 SpMV of the mixed paths."""
+        x, px = _arr(x, np.float32)
+        y = np.empty_like(x)
+        check(self._lib.cgx_inner_matvec(self._h, px, y.ctypes.data_as(C.c_void_p)))
+        return y
 
     # --- learned preconditioner ---
     def update_crs_values(self, value):

@@ -22,6 +22,7 @@
 #include <vector>
 
 #include "cgx.h"
+#include "band.cuh"
 #include "kernels.cuh"
 #include "learned.cuh"
 #include "sell.cuh"
@@ -130,6 +131,21 @@ static void sellu_free(SellU &S) {
   S = SellU{};
 }
 
+// Symmetric band copy of A's FP32 values (band.cuh). K > 0: the offsets of
+// A fit the layout (planned once per pattern); ok: the values of the last
+// refresh passed the symmetry check and U holds them.
+struct Band {
+  float *U = nullptr;
+  int K = 0;
+  int d[kBandMaxK] = {};
+  bool ok = false;
+};
+
+static void band_free(Band &B) {
+  if (B.U) cudaFree(B.U);
+  B = Band{};
+}
+
 struct cgx_handle {
   int device = 0;
   int num_sms = 148;
@@ -172,6 +188,9 @@ struct cgx_handle {
   SellU sa;
   float *sa_val = nullptr;
   bool sa_tried = false;
+  // Symmetric band copy, preferred over SELL-U when A fits it.
+  Band band;
+  bool band_tried = false;
 
   // Scratch: state, partial sums, dot result, validation flag.
   void *scratch = nullptr;
@@ -268,6 +287,8 @@ static void free_matrix(cgx_handle *h) {
   if (h->sa_val) cudaFree(h->sa_val);
   h->sa_val = nullptr;
   h->sa_tried = false;
+  band_free(h->band);
+  h->band_tried = false;
   h->format = -1;
   h->N = h->nz = 0;
   h->ptr = h->index = nullptr;
@@ -513,8 +534,26 @@ static cudaError_t launch_sellu(cgx_handle *h, const SellU &S, const VT *val,
              : launch_sellu_u<VT, 8, false>(h, A, x, op);
 }
 
+template <typename Op>
+static cudaError_t launch_band(cgx_handle *h, const float *x, Op op) {
+  BandView<4> B;
+  B.U = h->band.U;
+  B.N = h->N;
+  for (int k = 0; k < 4; k++) B.d[k] = k < h->band.K ? h->band.d[k] : 0;
+  auto kern = k_band<4, Op>;
+  int per_sm = 0;
+  cudaError_t e =
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, 0);
+  if (e != cudaSuccess) return e;
+  const int grid = std::max(1, std::min(std::min(h->num_sms * std::max(1, per_sm), kMaxGrid),
+                                        (h->N + kThreads - 1) / kThreads));
+  kern<<<grid, kThreads, 0, h->stream>>>(B, x, op, h->st, h->partials);
+  return cudaGetLastError();
+}
+
 static cudaError_t launch_inner_q(cgx_handle *h) {
   OpInnerQ op{h->p32, h->q32, ticket(h, kTicketInnerQ)};
+  if (h->band.ok) return launch_band(h, h->p32, op);
   if (h->sa.ok)
     return launch_sellu(h, h->sa, h->sa_val, h->p32, op);
   if (h->compact16)
@@ -838,6 +877,15 @@ cgx_status cgx_inner_layout(cgx_handle *h, long long *value_slots,
   if (value_slots) *value_slots = ok ? (long long)h->sa.slots : 0;
   if (uniform_slices) *uniform_slices = ok ? h->sa.uniform : 0;
   if (slices) *slices = ok ? (h->N + 31) / 32 : 0;
+  return CGX_SUCCESS;
+}
+
+cgx_status cgx_inner_band(cgx_handle *h, int *stored_offsets, int *offsets) {
+  if (!h) return fail(CGX_ERROR_INVALID_ARGUMENT, "handle is NULL");
+  const int K = h->band.ok ? h->band.K : 0;
+  if (stored_offsets) *stored_offsets = K;
+  if (offsets)
+    for (int k = 0; k < K; k++) offsets[k] = h->band.d[k];
   return CGX_SUCCESS;
 }
 
@@ -1333,6 +1381,88 @@ cgx_status build_sellu(cgx_handle *h, const int *ptr, const int *col,
                        size_t nnz, SellU &S);
 }
 
+// The offsets of A (k_band_offsets): B.K = 0 unless they form a symmetric
+// set with at most kBandMaxK non-negative members.
+static cgx_status band_plan(cgx_handle *h, Band &B) {
+  B = Band{};
+  const int N = h->N;
+  int *table = nullptr;
+  CUDA_TRY(cudaMalloc(&table, sizeof(int) * kBandTable));
+  std::vector<int> host(kBandTable, kBandEmpty);
+  int flag = 0;
+  cudaError_t e = cudaMemcpyAsync(table, host.data(), sizeof(int) * kBandTable,
+                                  cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(h->flag, 0, sizeof(int), h->stream);
+  if (e == cudaSuccess) {
+    k_band_offsets<<<grid_stream(h, N), kThreads, 0, h->stream>>>(
+        N, h->ptr, h->index, table, h->flag);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(host.data(), table, sizeof(int) * kBandTable,
+                        cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(&flag, h->flag, sizeof(int), cudaMemcpyDeviceToHost,
+                        h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  cudaFree(table);
+  CUDA_TRY(e);
+  if (flag) return CGX_SUCCESS;
+  std::vector<int> D;
+  for (int v : host)
+    if (v != kBandEmpty) D.push_back(v);
+  std::sort(D.begin(), D.end());
+  std::vector<int> up{0};
+  // |d| < N, so -d cannot overflow.
+  for (int d : D) {
+    if (!std::binary_search(D.begin(), D.end(), -d)) return CGX_SUCCESS;
+    if (d > 0) up.push_back(d);
+  }
+  if ((int)up.size() > kBandMaxK) return CGX_SUCCESS;
+  B.K = (int)up.size();
+  for (int k = 0; k < B.K; k++) B.d[k] = up[k];
+  return CGX_SUCCESS;
+}
+
+// U from A's current values and the symmetry check; B.ok if it passed.
+static cgx_status band_fill(cgx_handle *h, Band &B) {
+  const int N = h->N;
+  B.ok = false;
+  const size_t bytes = sizeof(float) * (size_t)N * kBandMaxK;
+  if (!B.U) CUDA_TRY(cudaMalloc(&B.U, bytes));
+  unsigned long long *counts = nullptr;
+  CUDA_TRY(cudaMalloc(&counts, 2 * sizeof(unsigned long long)));
+  BandOffsets o{};
+  o.K = B.K;
+  for (int k = 0; k < B.K; k++) o.d[k] = B.d[k];
+  unsigned long long hc[2] = {0, 0};
+  int flag = 0;
+  cudaError_t e = cudaMemsetAsync(B.U, 0, bytes, h->stream);
+  if (e == cudaSuccess)
+    e = cudaMemsetAsync(counts, 0, 2 * sizeof(unsigned long long), h->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(h->flag, 0, sizeof(int), h->stream);
+  if (e == cudaSuccess) {
+    k_band_fill<<<grid_stream(h, N), kThreads, 0, h->stream>>>(
+        N, h->ptr, h->index, h->value, o, B.U, counts, h->flag);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) {
+    k_band_check<<<grid_stream(h, N), kThreads, 0, h->stream>>>(
+        N, h->ptr, h->index, h->value, o, B.U, counts, h->flag);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(hc, counts, sizeof(hc), cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(&flag, h->flag, sizeof(int), cudaMemcpyDeviceToHost,
+                        h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  cudaFree(counts);
+  CUDA_TRY(e);
+  B.ok = flag == 0 && hc[0] == hc[1];
+  return CGX_SUCCESS;
+}
+
 static cgx_status ensure_f32(cgx_handle *h) {
   if (h->f32_valid) return CGX_SUCCESS;
   const int N = h->N;
@@ -1364,9 +1494,19 @@ static cgx_status ensure_f32(cgx_handle *h) {
   k_to_f32<<<grid_stream(h, N), kThreads, 0, h->stream>>>((size_t)N, h->C,
                                                           h->C32);
   CUDA_TRY(cudaGetLastError());
-  // SELL-U copy of A: the pattern once per matrix, the value array once it
-  // exists, the values on every refresh.
-  if (!h->sa_tried) {
+  // Symmetric band copy of A when it fits (planned once per pattern, filled
+  // and checked on every refresh); otherwise the SELL-U copy: the pattern
+  // once per matrix, the value array once it exists, the values on every
+  // refresh.
+  if (!h->band_tried) {
+    h->band_tried = true;
+    CGX_TRY(band_plan(h, h->band));
+  }
+  if (h->band.K > 0) {
+    CGX_TRY(band_fill(h, h->band));
+    if (!h->band.ok) band_free(h->band);
+  }
+  if (!h->band.ok && !h->sa_tried) {
     h->sa_tried = true;
     CGX_TRY(build_sellu(h, h->ptr, h->index, (size_t)h->nz, h->sa));
     // Mostly per-row slices (an irregular matrix) pad every row of a slice
@@ -2335,6 +2475,27 @@ cgx_status cgx_solve(cgx_handle *h, const cgx_options *opts,
   if (o.compute_true_residual && o.precision == CGX_PRECISION_FP64)
     CGX_TRY(cgx_true_residual(h, &res.true_residual));
   if (result) *result = res;
+  return CGX_SUCCESS;
+}
+
+cgx_status cgx_inner_matvec(cgx_handle *h, const float *x, float *y) {
+  CGX_TRY(need_matrix(h));
+  if (!x || !y) return fail(CGX_ERROR_INVALID_ARGUMENT, "x or y is NULL");
+  if (h->format != CGX_FORMAT_CRS)
+    return fail(CGX_ERROR_UNSUPPORTED, "the FP32 inner SpMV needs CRS");
+  DeviceGuard guard(h->device);
+  CGX_TRY(ensure_f32(h));
+  CGX_TRY(pull_state(h));
+  h->host_st->in_stop = 0;
+  h->host_st->in_finished = 0;
+  h->host_st->use_cond = 0;
+  CGX_TRY(push_state(h));
+  const size_t bytes = sizeof(float) * (size_t)h->N;
+  CUDA_TRY(cudaMemcpyAsync(h->p32, x, bytes, cudaMemcpyHostToDevice, h->stream));
+  CUDA_TRY(launch_inner_q(h));
+  CUDA_TRY(cudaMemcpyAsync(y, h->q32, bytes, cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  CGX_TRY(device_errors(h));
   return CGX_SUCCESS;
 }
 

@@ -1,0 +1,198 @@
+// Symmetric band layout for the FP32 inner SpMV of the mixed paths.
+//
+// It applies when every column offset col - row of A lies in one small set D
+// that is symmetric (d in D <=> -d in D) and A is symmetric. Then only the
+// diagonal and the upper half are stored: U[i][k] = A(i, i + d_k) for the K
+// non-negative offsets d_0 = 0 < d_1 < ... < d_{K-1} of D, zero where row i
+// has no such entry, row-major with K4 = 4 floats per row (one 16-byte
+// load). Row i's lower entries are read from the rows above it:
+// A(i, i - d_k) = A(i - d_k, i) = U[i - d_k][k]. The 7-point structured-grid
+// stencil fits (D = {0, +-1, +-n, +-n^2}): its values cost 16 bytes per row
+// instead of 28 (32 with SELL-U's padding), and the lower entries come from
+// rows the product read a moment earlier, which L1 and L2 still hold.
+//
+// Wider sets are left to SELL-U. On the 27-point stencil (14 stored
+// offsets), row-major rows of 64 bytes spread each warp's lower-entry loads
+// over 16 times the sectors they use (87 us per product at 128^3, against
+// 45.8 us for SELL-U), and a slot-major layout with coalesced loads only
+// tied SELL-U (45.6 us): with 62 loads per row instead of 35 the product is
+// bound by load issue, not by DRAM.
+//
+// The layout is built on the device from A's FP64 CRS (k_band_offsets,
+// k_band_fill, k_band_check) and used only if the check finds the FP32
+// values exactly symmetric, the pattern symmetric and no entry twice.
+#pragma once
+
+#include <climits>
+
+#include "device.cuh"
+
+namespace cgx {
+
+constexpr int kBandMaxK = 4;     // stored offsets (diagonal + upper)
+constexpr int kBandTable = 64;   // hash table of the distinct offsets
+constexpr int kBandEmpty = INT_MIN;
+
+template <int K4>
+struct BandView {
+  const float *U;  // N x K4, row-major
+  int N;
+  int d[K4];       // d[0] = 0 < d[1] < ... ; 0 for padding slots
+};
+
+// Offsets of D as the build kernels' argument.
+struct BandOffsets {
+  int K;
+  int d[kBandMaxK];
+};
+
+__device__ __forceinline__ unsigned band_hash(int d) {
+  return ((unsigned)d * 2654435761u) >> 26;  // 64 buckets
+}
+
+// Inserts d into a 64-entry open-addressing table; false if it is full.
+__device__ __forceinline__ bool band_insert(int *table, int d) {
+  unsigned h = band_hash(d);
+  for (int probe = 0; probe < kBandTable; probe++, h = (h + 1) & (kBandTable - 1)) {
+    const int v = *(volatile int *)&table[h];
+    if (v == d) return true;
+    if (v == kBandEmpty) {
+      const int old = atomicCAS(&table[h], kBandEmpty, d);
+      if (old == kBandEmpty || old == d) return true;
+    }
+  }
+  return false;
+}
+
+// Distinct offsets col - row of all entries, collected per CTA in shared
+// memory and merged into the global table. *flag |= 1 on overflow.
+__global__ void __launch_bounds__(kThreads)
+    k_band_offsets(int N, const int *__restrict__ ptr, const int *__restrict__ col,
+                   int *table, int *flag) {
+  __shared__ int local[kBandTable];
+  __shared__ int full;
+  if (threadIdx.x < kBandTable) local[threadIdx.x] = kBandEmpty;
+  if (threadIdx.x == 0) full = 0;
+  __syncthreads();
+  for (int i = blockIdx.x * kThreads + threadIdx.x; i < N; i += gridDim.x * kThreads) {
+    const int j1 = ptr[i + 1];
+    for (int j = ptr[i]; j < j1; j++)
+      if (!band_insert(local, col[j] - i)) {
+        full = 1;
+        break;
+      }
+  }
+  __syncthreads();
+  if (threadIdx.x < kBandTable && local[threadIdx.x] != kBandEmpty)
+    if (!band_insert(table, local[threadIdx.x])) atomicOr(flag, 1);
+  if (threadIdx.x == 0 && full) atomicOr(flag, 1);
+}
+
+__device__ __forceinline__ int band_slot(const BandOffsets &o, int d) {
+#pragma unroll
+  for (int k = 0; k < kBandMaxK; k++)
+    if (k < o.K && o.d[k] == d) return k;
+  return -1;
+}
+
+// U[i][k] = (float) A(i, i + d_k) for the diagonal and upper entries.
+// counts[0] += upper entries (d > 0). *flag |= 2 for an offset outside D
+// or an entry stored twice.
+__global__ void __launch_bounds__(kThreads)
+    k_band_fill(int N, const int *__restrict__ ptr, const int *__restrict__ col,
+                const double *__restrict__ val, BandOffsets o,
+                float *__restrict__ U, unsigned long long *counts, int *flag) {
+  unsigned long long upper = 0;
+  for (int i = blockIdx.x * kThreads + threadIdx.x; i < N; i += gridDim.x * kThreads) {
+    unsigned mask = 0;
+    const int j1 = ptr[i + 1];
+    for (int j = ptr[i]; j < j1; j++) {
+      const int d = col[j] - i;
+      if (d < 0) continue;
+      const int k = band_slot(o, d);
+      if (k < 0 || (mask >> k) & 1u) {
+        atomicOr(flag, 2);
+        continue;
+      }
+      mask |= 1u << k;
+      U[(size_t)i * kBandMaxK + k] = (float)val[j];
+      upper += d > 0;
+    }
+  }
+  for (int s = 16; s > 0; s >>= 1) upper += __shfl_xor_sync(0xffffffffu, upper, s);
+  if ((threadIdx.x & 31) == 0 && upper) atomicAdd(&counts[0], upper);
+}
+
+// Every lower entry A(i, i - d) must equal U[i - d][slot of d], once per
+// (i, d). counts[1] += lower entries; equal counts of upper and lower
+// entries then make the pairing one to one. *flag |= 4 on a mismatch or a
+// repeat.
+__global__ void __launch_bounds__(kThreads)
+    k_band_check(int N, const int *__restrict__ ptr, const int *__restrict__ col,
+                 const double *__restrict__ val, BandOffsets o,
+                 const float *__restrict__ U, unsigned long long *counts,
+                 int *flag) {
+  unsigned long long lower = 0;
+  for (int i = blockIdx.x * kThreads + threadIdx.x; i < N; i += gridDim.x * kThreads) {
+    unsigned mask = 0;
+    const int j1 = ptr[i + 1];
+    for (int j = ptr[i]; j < j1; j++) {
+      const int d = i - col[j];
+      if (d <= 0) continue;
+      const int k = band_slot(o, d);
+      if (k < 0 || (mask >> k) & 1u ||
+          U[(size_t)col[j] * kBandMaxK + k] != (float)val[j]) {
+        atomicOr(flag, 4);
+        continue;
+      }
+      mask |= 1u << k;
+      lower++;
+    }
+  }
+  for (int s = 16; s > 0; s >>= 1) lower += __shfl_xor_sync(0xffffffffu, lower, s);
+  if ((threadIdx.x & 31) == 0 && lower) atomicAdd(&counts[1], lower);
+}
+
+// FP32 SpMV on the band layout with the row epilogue of Op, one thread per
+// row: the row's own K4 values (one 16-byte load), the upper gathers of x,
+// and for each positive offset the value of the row d_k above and its x.
+// All loads are unconditional: padding slots hold value 0 with offset 0,
+// rows above row 0 are clamped to it and their products masked, and upper
+// columns past N - 1 (value 0) are clamped. x must be finite, as it is for
+// every operand of the inner solves.
+template <int K4, typename Op>
+__global__ void __launch_bounds__(kThreads)
+    k_band(BandView<K4> B, const float *__restrict__ x, Op op, CgState *st,
+           double *partials) {
+  static_assert(K4 == 4, "one row of the band layout is one float4");
+  if (op.skip(st)) return;
+  typename Op::Acc acc;
+  const int N = B.N;
+  const unsigned nmax = (unsigned)(N - 1);
+  for (int i = blockIdx.x * kThreads + threadIdx.x; i < N; i += gridDim.x * kThreads) {
+    const typename Op::Pre pre = op.prefetch(i);
+    const float4 u = __ldg(reinterpret_cast<const float4 *>(B.U) + i);
+    float xu[K4], lv[K4], xl[K4];
+#pragma unroll
+    for (int k = 0; k < K4; k++)
+      xu[k] = __ldg(&x[min((unsigned)i + (unsigned)B.d[k], nmax)]);
+#pragma unroll
+    for (int k = 1; k < K4; k++) {
+      const int j = i - B.d[k];
+      const int jc = max(j, 0);
+      lv[k] = __ldg(&B.U[(size_t)jc * K4 + k]);
+      xl[k] = __ldg(&x[jc]);
+      lv[k] = j < 0 ? 0.f : lv[k];
+    }
+    float sum = fmaf(u.x, xu[0], 0.f);
+    sum = fmaf(u.y, xu[1], sum);
+    sum = fmaf(u.z, xu[2], sum);
+    sum = fmaf(u.w, xu[3], sum);
+#pragma unroll
+    for (int k = 1; k < K4; k++) sum = fmaf(lv[k], xl[k], sum);
+    op.row(i, sum, acc, pre);
+  }
+  op.finish(acc, st, partials);
+}
+
+}  // namespace cgx

@@ -247,6 +247,23 @@ cgx_status cgx_true_residual(cgx_handle *h, double *rel);
 cgx_status cgx_time_spmv(cgx_handle *h, cgx_precision precision, int reps,
                          double *us_per_launch);
 
+/* Symmetric band form of A's FP32 copy (no counterpart in the reference):
+ * when A is symmetric and all its column offsets col - row form one
+ * symmetric set with at most 4 non-negative members (the 7-point
+ * structured-grid stencil: 0, 1, n, n^2), the inner SpMV stores per row
+ * only the values at those offsets (the diagonal and the upper half) and
+ * reads each lower entry from the row above that holds it.
+ * *stored_offsets = that count, or 0 when the inner SpMV uses another form
+ * (or the FP32 copy is not built yet); offsets (NULL, or room for 4)
+ * receives them, ascending from 0. */
+cgx_status cgx_inner_band(cgx_handle *h, int *stored_offsets, int *offsets);
+
+/* y = A x by the inner FP32 SpMV of the mixed and learned paths, on
+ * whichever form it uses (no counterpart in the reference; it exposes that
+ * product to tests): x and y are N host floats. Builds the FP32 copy if
+ * needed; overwrites the inner p and q and the solver scalars. CRS only. */
+cgx_status cgx_inner_matvec(cgx_handle *h, const float *x, float *y);
+
 /* Layout of A's FP32 copy used by the inner SpMV of the mixed and learned
  * paths (built by the first mixed solve; no counterpart in the reference):
  * rows in slices of 32, *slices in all, *uniform_slices of them storing one

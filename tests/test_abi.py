@@ -60,6 +60,8 @@ def test_errors_are_statuses():
     lib = cg.load()
     assert lib.cgx_gnn_set_probes(None, 0, 0, 1.0, 0) == 1
     assert lib.cgx_learned_capture_residual(None, 0) == 1
+    assert lib.cgx_inner_band(None, None, None) == 1
+    assert lib.cgx_inner_matvec(None, None, None) == 1
     with pytest.raises(cg.CgxError) as e:
         _lib.check(lib.cgx_create(C.byref(C.c_void_p()), -1))
     assert e.value.status == 1

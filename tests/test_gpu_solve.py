@@ -159,21 +159,86 @@ def _shuffle_rows(A, seed):
     return G.Crs(A.N, A.ptr, index, value)
 
 
-@pytest.mark.parametrize("case", ["ragged", "unsorted", "wide", "stencil27_odd"])
-def test_mixed_on_irregular_patterns(handle, case):
-    """The FP32 inner SpMV on both of its forms: the SELL-U layout for a
-    stencil (uniform slices with zero-filled missing neighbours at the
-    boundary, a last slice shorter than 32 rows) and FP32 CRS for matrices
-    whose slices would be mostly per-row (ragged random rows, rows whose
-    offsets span more than 32 slots, unsorted rows)."""
+def _asymmetric(A, rel=1e-4):
+    """A with the entry above the diagonal in row N/2 scaled by 1 + rel: no
+    longer exactly symmetric, close enough for CG to converge."""
+    value = A.value.copy()
+    i = A.N // 2
+    a, b = A.ptr[i], A.ptr[i + 1]
+    j = a + int(np.nonzero(A.index[a:b] > i)[0][0])
+    value[j] *= 1.0 + rel
+    return G.Crs(A.N, A.ptr, A.index, value)
+
+
+# Inner SpMV form per case: the symmetric band for the 7-point stencil
+# (unsorted rows included), SELL-U for the 27-point stencil (14 stored
+# offsets) and for a 7-point stencil whose values are not exactly symmetric,
+# FP32 CRS for matrices whose slices would be mostly per-row.
+_IRREGULAR = {
+    "ragged": "crs",
+    "unsorted": "band",
+    "wide": "crs",
+    "stencil27_odd": "sellu",
+    "stencil7_asym": "sellu",
+}
+
+
+def _irregular_matrix(case):
     if case == "ragged":
-        A = random_crs(1007, max_len=12, seed=3, spd=True)
-    elif case == "unsorted":
-        A = _shuffle_rows(G.diffusion3d(13, stencil=7, seed=4), seed=5)
-    elif case == "wide":
-        A = random_crs(777, max_len=80, seed=4, spd=True)
+        return random_crs(1007, max_len=12, seed=3, spd=True)
+    if case == "unsorted":
+        return _shuffle_rows(G.diffusion3d(13, stencil=7, seed=4), seed=5)
+    if case == "wide":
+        return random_crs(777, max_len=80, seed=4, spd=True)
+    if case == "stencil27_odd":
+        return G.diffusion3d(11, stencil=27, seed=6)
+    return _asymmetric(G.diffusion3d(11, stencil=7, seed=6))
+
+
+def _check_inner_form(handle, A, form):
+    slots, uniform, slices = handle.inner_layout()
+    band = handle.inner_band()
+    if form == "band":
+        n = round(A.N ** (1 / 3))
+        assert band == [0, 1, n, n * n] and slots == 0
+    elif form == "sellu":
+        assert band == [] and slices == (A.N + 31) // 32 and uniform == slices
+        assert slots >= A.nz
     else:
-        A = G.diffusion3d(11, stencil=27, seed=6)
+        assert band == [] and slots == 0
+
+
+@pytest.mark.parametrize("case", sorted(_IRREGULAR))
+def test_inner_product_on_every_form(handle, case):
+    """y = A x by the FP32 inner SpMV, on each of its forms, against the FP64
+    product of the same FP32 x: within 4e-6 of sum |a_ij x_j| per row. x has
+    large entries at both ends, where the band form masks the rows above row
+    0 and clamps the columns past N - 1."""
+    A = _irregular_matrix(case)
+    handle.upload_crs(A.ptr, A.index, A.value)
+    handle.upload_jacobi(1.0 / A.diagonal())
+    x = np.random.default_rng(11).standard_normal(A.N).astype(np.float32)
+    x[:3] = 1e3
+    x[-3:] = -1e3
+    y = handle.inner_matvec(x)
+    _check_inner_form(handle, A, _IRREGULAR[case])
+    xd = x.astype(np.float64)
+    ref = A.matvec(xd)
+    absA = G.Crs(A.N, A.ptr, A.index, np.abs(A.value))
+    bound = 4e-6 * absA.matvec(np.abs(xd)) + 1e-30
+    assert np.all(np.abs(y.astype(np.float64) - ref) <= bound)
+
+
+@pytest.mark.parametrize("case", sorted(_IRREGULAR))
+def test_mixed_on_irregular_patterns(handle, case):
+    """The mixed solve on every form of the FP32 inner SpMV: the symmetric
+    band for the 7-point stencil (rows stored out of order), SELL-U for the
+    27-point stencil and when the values are not exactly symmetric (uniform
+    slices with zero-filled missing neighbours at the boundary, a last slice
+    shorter than 32 rows), and FP32 CRS for matrices whose slices would be
+    mostly per-row (ragged random rows, rows whose offsets span more than 32
+    slots)."""
+    A = _irregular_matrix(case)
     b, _ = G.rhs_for(A, seed=7)
     handle.upload_crs(A.ptr, A.index, A.value)
     Cd = 1.0 / A.diagonal()
@@ -187,13 +252,7 @@ def test_mixed_on_irregular_patterns(handle, case):
     assert tr <= 1e-9
     _, it_o, outer_o, _ = O.mixed_ir_solve(A.ptr, A.index, A.value, Cd, b)
     assert abs(res["iterations"] - it_o) <= 0.05 * it_o + 2
-    # A stencil keeps the SELL-U layout (every slice uniform); matrices whose
-    # slices are mostly per-row run the inner SpMV on FP32 CRS.
-    slots, uniform, slices = handle.inner_layout()
-    if case == "stencil27_odd":
-        assert slices == (A.N + 31) // 32 and uniform == slices and slots >= A.nz
-    else:
-        assert slots == 0
+    _check_inner_form(handle, A, _IRREGULAR[case])
 
 
 def test_time_spmv_measures_the_fused_product(handle):
