@@ -106,6 +106,7 @@ PROTOTYPES = {
     "cgx_inner_layout": [_P, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),
                          C.POINTER(C.c_longlong)],
     "cgx_inner_band": [_P, _PI, _PI],
+    "cgx_learned_apply": [_P, _P, _P],
     "cgx_inner_matvec": [_P, _P, _P],
     "cgx_mtx_read": [C.c_char_p, _PI, _PI, C.POINTER(_PI), C.POINTER(_PI),
                      C.POINTER(_PD)],
@@ -339,6 +340,13 @@ class Handle:
 
     def learned_factor(self, gnn, eps=0.0):
         check(self._lib.cgx_learned_factor(self._h, gnn._g, float(eps)))
+
+    def learned_apply(self, r):
+        """z = G (G^T r) + eps C r (float32), as the inner solve applies it."""
+        r, pr = _arr(r, np.float32)
+        z = np.empty_like(r)
+        check(self._lib.cgx_learned_apply(self._h, pr, z.ctypes.data_as(C.c_void_p)))
+        return z
 
     def learned_get_factor(self):
         """(ghat, rows, cols) of the unscaled factor on its pattern."""

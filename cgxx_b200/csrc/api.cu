@@ -228,6 +228,13 @@ struct Learned {
   void *sell_val = nullptr;
   __nv_bfloat16 *sg_val = nullptr, *st_val = nullptr;
   bool sell_ok = false;
+  // Band copy of G (band.cuh) when A's offsets fit the band: preferred over
+  // the SELL-U copies, which are then not built.
+  void *gb_mem = nullptr;
+  __nv_bfloat16 *gb_val = nullptr;
+  int *g2b = nullptr;
+  int gb_d[kBandMaxK] = {};
+  bool gb_ok = false;
   __nv_bfloat16 *h[4] = {};
   __nv_bfloat16 *agg[3] = {};
   float *pre[4] = {};
@@ -272,6 +279,7 @@ static void free_learned(cgx_handle *h) {
   sellu_free(h->L->sg);
   sellu_free(h->L->st);
   if (h->L->sell_val) cudaFree(h->L->sell_val);
+  if (h->L->gb_mem) cudaFree(h->L->gb_mem);
   delete h->L;
   h->L = nullptr;
 }
@@ -1550,12 +1558,34 @@ static cgx_status true_residual_r2(cgx_handle *h, double *r2) {
   return CGX_SUCCESS;
 }
 
+template <bool TRANS, typename Op>
+static cudaError_t launch_gband(cgx_handle *h, const float *x, Op op) {
+  GBandView B;
+  B.val = h->L->gb_val;
+  B.N = h->N;
+  for (int k = 0; k < kBandMaxK; k++) B.d[k] = h->L->gb_d[k];
+  auto kern = k_gband<TRANS, Op>;
+  int per_sm = 0;
+  cudaError_t e =
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, 0);
+  if (e != cudaSuccess) return e;
+  const int grid = std::max(1, std::min(std::min(h->num_sms * std::max(1, per_sm), kMaxGrid),
+                                        (h->N + kThreads - 1) / kThreads));
+  kern<<<grid, kThreads, 0, h->stream>>>(B, x, op, h->st, h->partials);
+  return cudaGetLastError();
+}
+
 // z = G (G^T r) + eps C r with <r,z> (start: also p = z and rho).
 static cudaError_t launch_learned_apply(cgx_handle *h, bool start) {
   Learned *L = h->L;
   const OpLearnedZ zop{h->r32, h->C32, L->z32, h->p32, L->eps, start ? 1 : 0,
                        ticket(h, kTicketInnerStart)};
   cudaError_t e;
+  if (L->gb_ok) {
+    e = launch_gband<true>(h, h->r32, OpInnerStore{L->y32});
+    if (e != cudaSuccess) return e;
+    return launch_gband<false>(h, L->y32, zop);
+  }
   if (L->sell_ok) {
     e = launch_sellu(h, L->st, L->st_val, h->r32, OpInnerStore{L->y32});
     if (e != cudaSuccess) return e;
@@ -1967,6 +1997,42 @@ cgx_status build_sellu(cgx_handle *h, const int *ptr, const int *col,
 cgx_status build_sell(cgx_handle *h) {
   Learned *L = h->L;
   L->sell_ok = false;
+  L->gb_ok = false;
+  if (L->gb_mem) cudaFree(L->gb_mem);
+  L->gb_mem = nullptr;
+  // The band copy when A's offsets fit it.
+  Band plan;
+  CGX_TRY(band_plan(h, plan));
+  if (plan.K > 0) {
+    const int N = h->N;
+    Carver c;
+    size_t o_v = take_n<__nv_bfloat16>(c, (size_t)N * kBandMaxK);
+    size_t o_m = take_n<int>(c, (size_t)L->nnzL);
+    CUDA_TRY(cudaMalloc(&L->gb_mem, c.off));
+    L->gb_val = (__nv_bfloat16 *)((char *)L->gb_mem + o_v);
+    L->g2b = (int *)((char *)L->gb_mem + o_m);
+    BandOffsets o{};
+    o.K = plan.K;
+    for (int k = 0; k < kBandMaxK; k++) {
+      o.d[k] = plan.d[k];
+      L->gb_d[k] = k < plan.K ? plan.d[k] : 0;
+    }
+    CUDA_TRY(cudaMemsetAsync(L->gb_mem, 0, c.off, h->stream));
+    CUDA_TRY(cudaMemsetAsync(h->flag, 0, sizeof(int), h->stream));
+    k_gband_map<<<grid_stream(h, L->nnzL), kThreads, 0, h->stream>>>(
+        L->nnzL, L->grow, L->gcol, o, L->g2b, h->flag);
+    CUDA_TRY(cudaGetLastError());
+    int flag = 0;
+    CUDA_TRY(cudaMemcpyAsync(&flag, h->flag, sizeof(int), cudaMemcpyDeviceToHost,
+                             h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    if (flag == 0) {
+      L->gb_ok = true;
+      return CGX_SUCCESS;
+    }
+    cudaFree(L->gb_mem);
+    L->gb_mem = nullptr;
+  }
   CGX_TRY(build_sellu(h, L->gptr, L->gcol, (size_t)L->nnzL, L->sg));
   CGX_TRY(build_sellu(h, L->tptr, L->tcol, (size_t)L->nnzL, L->st));
   if (!L->sg.ok || !L->st.ok) return CGX_SUCCESS;
@@ -2007,7 +2073,8 @@ cudaError_t gnn_forward(cgx_handle *h, const float *P, bool scaled) {
       L->nnzL, L->grow, L->gcol, L->g2a, L->ahat, L->o, L->ghat, L->dis,
       L->g2t, scaled ? L->gs : nullptr, scaled ? L->gts : nullptr,
       scaled && L->sell_ok ? L->sg_val : nullptr,
-      scaled && L->sell_ok ? L->st_val : nullptr, L->sg.map, L->st.map);
+      scaled && L->sell_ok ? L->st_val : nullptr, L->sg.map, L->st.map,
+      scaled && L->gb_ok ? L->gb_val : nullptr, L->g2b);
   return cudaGetLastError();
 }
 
@@ -2281,6 +2348,29 @@ cgx_status cgx_learned_factor(cgx_handle *h, cgx_gnn *gn, double eps) {
   CUDA_TRY(gnn_forward(h, gn->params, true));
   h->L->eps = (float)eps;
   h->L->has_factor = true;
+  return CGX_SUCCESS;
+}
+
+cgx_status cgx_learned_apply(cgx_handle *h, const float *r, float *z) {
+  CGX_TRY(need_matrix(h));
+  if (!r || !z) return fail(CGX_ERROR_INVALID_ARGUMENT, "r or z is NULL");
+  if (!h->L || !h->L->has_factor)
+    return fail(CGX_ERROR_INVALID_STATE, "call cgx_learned_factor first");
+  if (!h->c_valid)
+    return fail(CGX_ERROR_INVALID_STATE, "Jacobi preconditioner not set");
+  DeviceGuard guard(h->device);
+  CGX_TRY(ensure_f32(h));
+  CGX_TRY(pull_state(h));
+  h->host_st->in_stop = 0;
+  h->host_st->in_finished = 0;
+  h->host_st->use_cond = 0;
+  CGX_TRY(push_state(h));
+  const size_t bytes = sizeof(float) * (size_t)h->N;
+  CUDA_TRY(cudaMemcpyAsync(h->r32, r, bytes, cudaMemcpyHostToDevice, h->stream));
+  CUDA_TRY(launch_learned_apply(h, true));
+  CUDA_TRY(cudaMemcpyAsync(z, h->L->z32, bytes, cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  CGX_TRY(device_errors(h));
   return CGX_SUCCESS;
 }
 

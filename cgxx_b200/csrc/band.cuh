@@ -23,6 +23,8 @@
 // values exactly symmetric, the pattern symmetric and no entry twice.
 #pragma once
 
+#include <cuda_bf16.h>
+
 #include <climits>
 
 #include "device.cuh"
@@ -190,6 +192,85 @@ __global__ void __launch_bounds__(kThreads)
     sum = fmaf(u.w, xu[3], sum);
 #pragma unroll
     for (int k = 1; k < K4; k++) sum = fmaf(lv[k], xl[k], sum);
+    op.row(i, sum, acc, pre);
+  }
+  op.finish(acc, st, partials);
+}
+
+// ---------------------------------------------------------------------------
+// The learned factor G on the band: G lies on A's lower triangle, so its
+// column offsets are 0, -d_1, ..., -d_{K-1}, and one BF16 array
+// Gb[i][k] = G(i, i - d_k) (8 bytes per row, zero where row i has no such
+// entry) serves both products of the apply:
+//   z = G y:    z_i = sum_k Gb[i][k] y[i - d_k]          (the row's own values)
+//   y = G^T r:  y_i = sum_k Gb[i + d_k][k] r[i + d_k]    (values of the rows below)
+// Neither needs slice descriptors or offset loads: one memory round trip
+// per row.
+
+struct GBandView {
+  const __nv_bfloat16 *val;  // N x 4, row-major
+  int N;
+  int d[kBandMaxK];          // 0 for padding slots
+};
+
+// Slot of every entry of G (CRS order): map[e] = 4 i + k for the entry
+// (i, i - d_k). *flag |= 8 for an offset that is not one of -d_k.
+__global__ void __launch_bounds__(kThreads)
+    k_gband_map(int nnz, const int *__restrict__ grow, const int *__restrict__ gcol,
+                BandOffsets o, int *__restrict__ map, int *flag) {
+  for (int e = blockIdx.x * kThreads + threadIdx.x; e < nnz; e += gridDim.x * kThreads) {
+    const int i = grow[e];
+    const int k = band_slot(o, i - gcol[e]);
+    if (k < 0) {
+      atomicOr(flag, 8);
+      map[e] = 4 * i;
+    } else {
+      map[e] = 4 * i + k;
+    }
+  }
+}
+
+__device__ __forceinline__ float bf16_bits_to_float(unsigned short b) {
+  return __uint_as_float((unsigned)b << 16);
+}
+
+// TRANS = false: z = G x; TRANS = true: y = G^T x; with the row epilogue of
+// Op. Gathers are clamped into [0, N); a clamped slot's value is 0 (G) or
+// masked (G^T, rows below N - 1). x must be finite.
+template <bool TRANS, typename Op>
+__global__ void __launch_bounds__(kThreads)
+    k_gband(GBandView B, const float *__restrict__ x, Op op, CgState *st,
+            double *partials) {
+  if (op.skip(st)) return;
+  typename Op::Acc acc;
+  const int N = B.N;
+  const unsigned short *gv = reinterpret_cast<const unsigned short *>(B.val);
+  for (int i = blockIdx.x * kThreads + threadIdx.x; i < N; i += gridDim.x * kThreads) {
+    const typename Op::Pre pre = op.prefetch(i);
+    float v[kBandMaxK], xv[kBandMaxK];
+    if (!TRANS) {
+      const uint2 raw = __ldg(reinterpret_cast<const uint2 *>(B.val) + i);
+      v[0] = __uint_as_float(raw.x << 16);
+      v[1] = __uint_as_float(raw.x & 0xffff0000u);
+      v[2] = __uint_as_float(raw.y << 16);
+      v[3] = __uint_as_float(raw.y & 0xffff0000u);
+#pragma unroll
+      for (int k = 0; k < kBandMaxK; k++) xv[k] = __ldg(&x[max(i - B.d[k], 0)]);
+    } else {
+      v[0] = bf16_bits_to_float(__ldg(&gv[(size_t)i * 4]));
+      xv[0] = __ldg(&x[i]);
+#pragma unroll
+      for (int k = 1; k < kBandMaxK; k++) {
+        const unsigned j = (unsigned)i + (unsigned)B.d[k];
+        const int jc = (int)min(j, (unsigned)(N - 1));
+        v[k] = bf16_bits_to_float(__ldg(&gv[(size_t)jc * 4 + k]));
+        xv[k] = __ldg(&x[jc]);
+        v[k] = j < (unsigned)N ? v[k] : 0.f;
+      }
+    }
+    float sum = 0.f;
+#pragma unroll
+    for (int k = 0; k < kBandMaxK; k++) sum = fmaf(v[k], xv[k], sum);
     op.row(i, sum, acc, pre);
   }
   op.finish(acc, st, partials);

@@ -426,7 +426,9 @@ __global__ void k_assemble(int nnzL, const int *__restrict__ grow,
                            float *__restrict__ gts, __nv_bfloat16 *__restrict__ sgv,
                            __nv_bfloat16 *__restrict__ stv,
                            const int *__restrict__ g2sg,
-                           const int *__restrict__ t2st) {
+                           const int *__restrict__ t2st,
+                           __nv_bfloat16 *__restrict__ gbv,
+                           const int *__restrict__ g2b) {
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nnzL;
        e += gridDim.x * blockDim.x) {
     const int i = grow[e], j = gcol[e];
@@ -441,7 +443,9 @@ __global__ void k_assemble(int nnzL, const int *__restrict__ grow,
       v = fabsf(ahat[g2a[e]]) * (1.f + o[i * NOUT + 0] + uv);
     }
     ghat[e] = v;
-    if (sgv) {  // the SELL-U copies of G and G^T (BF16)
+    if (gbv) {  // the band copy of G (BF16), which serves G and G^T
+      gbv[g2b[e]] = __float2bfloat16_rn((float)(dis[i] * (double)v));
+    } else if (sgv) {  // the SELL-U copies of G and G^T (BF16)
       const __nv_bfloat16 bv = __float2bfloat16_rn((float)(dis[i] * (double)v));
       sgv[g2sg[e]] = bv;
       stv[t2st[g2t[e]]] = bv;

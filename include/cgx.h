@@ -205,6 +205,12 @@ cgx_status cgx_learned_factor(cgx_handle *h, cgx_gnn *g, double eps);
  * each optional). */
 cgx_status cgx_learned_get_factor(cgx_handle *h, int *nnzL, float *ghat,
                                   int *rows, int *cols);
+/* z = G (G^T r) + eps C r, the learned preconditioner as the inner solve
+ * applies it (BF16 factor values, FP32 vectors), on N host floats (no
+ * counterpart in the reference; it exposes that product to tests). Needs
+ * cgx_learned_factor and the Jacobi vector C; overwrites the inner vectors
+ * and the solver scalars. */
+cgx_status cgx_learned_apply(cgx_handle *h, const float *r, float *z);
 /* Probe recipe of the network's training (no counterpart in the reference),
  * for the 8 probe columns: the last `residual_cols` are the handle's
  * residual snapshots (cgx_learned_capture_residual; they must exist for the

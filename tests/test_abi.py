@@ -62,6 +62,7 @@ def test_errors_are_statuses():
     assert lib.cgx_learned_capture_residual(None, 0) == 1
     assert lib.cgx_inner_band(None, None, None) == 1
     assert lib.cgx_inner_matvec(None, None, None) == 1
+    assert lib.cgx_learned_apply(None, None, None) == 1
     with pytest.raises(cg.CgxError) as e:
         _lib.check(lib.cgx_create(C.byref(C.c_void_p()), -1))
     assert e.value.status == 1

@@ -72,6 +72,44 @@ def test_factor_matches_oracle(name, make):
     net.close()
 
 
+@pytest.mark.parametrize("name,make", MATRICES + [
+    ("diffusion7_13", lambda: G.diffusion3d(13, 7, sigma=1.0, corr_len=4.0, seed=5)),
+], ids=[m[0] for m in MATRICES] + ["diffusion7_13"])
+def test_apply_matches_factor(name, make):
+    """z = G (G^T r) + eps C r from the device (BF16 factor values, the band
+    copy of G for the 7-point stencils, SELL-U or FP32 CRS otherwise)
+    against the same product in FP64 from the factor the device reports:
+    within 1.6e-2 of (|G| |G|^T |r|)_i + eps C_i |r_i| per row (two BF16
+    roundings of the factor values, 2^-9 each, and FP32 sums)."""
+    A = make()
+    h = _setup(A)
+    net = cg.Gnn(0, _params(3))
+    eps = 1e-3
+    h.learned_factor(net, eps)
+    ghat, rows, cols = h.learned_get_factor()
+    dis = 1.0 / np.sqrt(A.diagonal())
+    gv = dis[rows] * ghat.astype(np.float64)
+
+    def g_times(v, x):  # G x
+        return np.bincount(rows, weights=v * x[cols], minlength=A.N)
+
+    def gt_times(v, x):  # G^T x
+        return np.bincount(cols, weights=v * x[rows], minlength=A.N)
+
+    C = 1.0 / A.diagonal()
+    rng = np.random.default_rng(4)
+    for _ in range(2):
+        r = rng.standard_normal(A.N).astype(np.float32)
+        z = h.learned_apply(r)
+        rd = r.astype(np.float64)
+        ref = g_times(gv, gt_times(gv, rd)) + eps * C * rd
+        ga = np.abs(gv)
+        bound = 1.6e-2 * g_times(ga, gt_times(ga, np.abs(rd))) + 1e-6 * eps * C * np.abs(rd)
+        assert np.all(np.abs(z - ref) <= bound + 1e-30)
+    h.close()
+    net.close()
+
+
 @pytest.mark.parametrize("name,make", MATRICES, ids=[m[0] for m in MATRICES])
 def test_gradient_matches_oracle(name, make):
     A = make()
