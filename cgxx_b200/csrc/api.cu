@@ -19,6 +19,8 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <map>
+#include <unordered_map>
 #include <vector>
 
 #include "cgx.h"
@@ -126,8 +128,12 @@ struct SellU {
   bool ok = false;
 };
 
-static void sellu_free(SellU &S) {
-  if (S.mem) cudaFree(S.mem);
+struct cgx_handle;
+static cudaError_t dev_alloc(cgx_handle *h, void **p, size_t bytes);
+static void dev_free(cgx_handle *h, void *p);
+
+static void sellu_free(cgx_handle *h, SellU &S) {
+  if (S.mem) dev_free(h, S.mem);
   S = SellU{};
 }
 
@@ -141,13 +147,18 @@ struct Band {
   bool ok = false;
 };
 
-static void band_free(Band &B) {
-  if (B.U) cudaFree(B.U);
+static void band_free(cgx_handle *h, Band &B) {
+  if (B.U) dev_free(h, B.U);
   B = Band{};
 }
 
 struct cgx_handle {
   int device = 0;
+  // Device blocks of replaced matrices, kept for the next upload
+  // (dev_alloc / dev_free): size -> block, and the size of every block the
+  // handle owns.
+  std::multimap<size_t, void *> spare;
+  std::unordered_map<void *, size_t> block_size;
   int num_sms = 148;
   cudaStream_t own_stream = nullptr;
   cudaStream_t stream = nullptr;
@@ -264,6 +275,53 @@ struct cgx_gnn {
   float smooth_scale = 1.f;
 };
 
+// Device memory of a handle. A block released by dev_free stays with the
+// handle, and dev_alloc hands it out again for a request it fits (at most a
+// quarter plus 1 MiB larger): re-uploading a matrix of the same size, as a
+// time-stepping caller does every step, then allocates nothing, where
+// cudaMalloc and cudaFree of the same gigabytes took 8 to 180 ms per upload.
+// All of a handle's work is ordered on its stream (cgx_set_stream first
+// drains the old one), so a block is never reused while a kernel still
+// reads it. On an allocation failure the spare blocks are released and the
+// allocation is retried; cgx_destroy releases everything.
+static void release_spare(cgx_handle *h) {
+  for (auto &kv : h->spare) {
+    h->block_size.erase(kv.second);
+    cudaFree(kv.second);
+  }
+  h->spare.clear();
+}
+
+static cudaError_t dev_alloc(cgx_handle *h, void **p, size_t bytes) {
+  *p = nullptr;
+  if (bytes == 0) bytes = 1;
+  auto it = h->spare.lower_bound(bytes);
+  if (it != h->spare.end() && it->first <= bytes + bytes / 4 + (1u << 20)) {
+    *p = it->second;
+    h->spare.erase(it);
+    return cudaSuccess;
+  }
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e == cudaErrorMemoryAllocation && !h->spare.empty()) {
+    cudaGetLastError();
+    release_spare(h);
+    e = cudaMalloc(p, bytes);
+  }
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    return e;
+  }
+  h->block_size[*p] = bytes;
+  return cudaSuccess;
+}
+
+static void dev_free(cgx_handle *h, void *p) {
+  if (!p) return;
+  auto it = h->block_size.find(p);
+  if (it == h->block_size.end()) return;
+  h->spare.emplace(it->second, p);
+}
+
 static void drop_graphs(cgx_handle *h) {
   for (auto &g : h->graphs) {
     if (g.exec) cudaGraphExecDestroy(g.exec);
@@ -274,12 +332,12 @@ static void drop_graphs(cgx_handle *h) {
 
 static void free_learned(cgx_handle *h) {
   if (!h->L) return;
-  if (h->L->mem) cudaFree(h->L->mem);
-  if (h->L->train) cudaFree(h->L->train);
-  sellu_free(h->L->sg);
-  sellu_free(h->L->st);
-  if (h->L->sell_val) cudaFree(h->L->sell_val);
-  if (h->L->gb_mem) cudaFree(h->L->gb_mem);
+  if (h->L->mem) dev_free(h, h->L->mem);
+  if (h->L->train) dev_free(h, h->L->train);
+  sellu_free(h, h->L->sg);
+  sellu_free(h, h->L->st);
+  if (h->L->sell_val) dev_free(h, h->L->sell_val);
+  if (h->L->gb_mem) dev_free(h, h->L->gb_mem);
   delete h->L;
   h->L = nullptr;
 }
@@ -287,15 +345,15 @@ static void free_learned(cgx_handle *h) {
 static void free_matrix(cgx_handle *h) {
   drop_graphs(h);
   free_learned(h);
-  if (h->mat_mem) cudaFree(h->mat_mem);
-  if (h->vec_mem) cudaFree(h->vec_mem);
-  if (h->f32_mem) cudaFree(h->f32_mem);
+  if (h->mat_mem) dev_free(h, h->mat_mem);
+  if (h->vec_mem) dev_free(h, h->vec_mem);
+  if (h->f32_mem) dev_free(h, h->f32_mem);
   h->mat_mem = h->vec_mem = h->f32_mem = nullptr;
-  sellu_free(h->sa);
-  if (h->sa_val) cudaFree(h->sa_val);
+  sellu_free(h, h->sa);
+  if (h->sa_val) dev_free(h, h->sa_val);
   h->sa_val = nullptr;
   h->sa_tried = false;
-  band_free(h->band);
+  band_free(h, h->band);
   h->band_tried = false;
   h->format = -1;
   h->N = h->nz = 0;
@@ -838,6 +896,7 @@ cgx_status cgx_destroy(cgx_handle *h) {
   DeviceGuard guard(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
   free_matrix(h);
+  release_spare(h);
   for (auto &ev : h->ev)
     if (ev) cudaEventDestroy(ev);
   for (auto &ev : h->evpool) cudaEventDestroy(ev);
@@ -853,6 +912,9 @@ cgx_status cgx_set_stream(cgx_handle *h, void *stream) {
   if (!h) return fail(CGX_ERROR_INVALID_ARGUMENT, "handle is NULL");
   cudaStream_t s = stream ? (cudaStream_t)stream : h->own_stream;
   if (s != h->stream) {
+    DeviceGuard guard(h->device);
+    // Blocks the handle reuses were last used on the old stream.
+    if (h->stream) CUDA_TRY(cudaStreamSynchronize(h->stream));
     drop_graphs(h);
     h->stream = s;
   }
@@ -913,7 +975,7 @@ static cgx_status alloc_vectors(cgx_handle *h, int N) {
   Carver c;
   size_t o[8];
   for (int i = 0; i < 8; i++) o[i] = c.take<double>((size_t)N + kPad);
-  CUDA_TRY(cudaMalloc(&h->vec_mem, c.off));
+  CUDA_TRY(dev_alloc(h, (void **)&h->vec_mem, c.off));
   char *base = (char *)h->vec_mem;
   for (int i = 0; i < 6; i++) h->vec[i] = (double *)(base + o[i]);
   h->C = (double *)(base + o[6]);
@@ -970,7 +1032,7 @@ static cgx_status upload_rows(cgx_handle *h, int N, int nz, const int *ptr,
   size_t o_ptr = c.take<int>((size_t)N + 1 + kPad);
   size_t o_idx = c.take<int>((size_t)nz + kPad);
   size_t o_val = c.take<double>((size_t)nz + kPad);
-  CUDA_TRY(cudaMalloc(&h->mat_mem, c.off));
+  CUDA_TRY(dev_alloc(h, (void **)&h->mat_mem, c.off));
   char *base = (char *)h->mat_mem;
   h->ptr = (int *)(base + o_ptr);
   h->index = (int *)(base + o_idx);
@@ -1024,7 +1086,7 @@ cgx_status cgx_upload_ell(cgx_handle *h, int N, int nz, int maxNz,
   size_t o_len = c.take<int>((size_t)N + kPad);
   size_t o_idx = c.take<int>(elems + kPad);
   size_t o_dat = c.take<double>(elems + kPad);
-  CUDA_TRY(cudaMalloc(&h->mat_mem, c.off));
+  CUDA_TRY(dev_alloc(h, (void **)&h->mat_mem, c.off));
   char *base = (char *)h->mat_mem;
   h->ell_length = (int *)(base + o_len);
   h->ell_index = (int *)(base + o_idx);
@@ -1037,7 +1099,7 @@ cgx_status cgx_upload_ell(cgx_handle *h, int N, int nz, int maxNz,
     void *tmp = nullptr;
     Carver t;
     const size_t o_ti = t.take<int>(celems), o_td = t.take<double>(celems);
-    CUDA_TRY(cudaMalloc(&tmp, t.off));
+    CUDA_TRY(dev_alloc(h, (void **)&tmp, t.off));
     int *ci = (int *)((char *)tmp + o_ti);
     double *cd = (double *)((char *)tmp + o_td);
     cudaError_t e = cudaMemcpyAsync(ci, index, sizeof(int) * celems,
@@ -1051,7 +1113,7 @@ cgx_status cgx_upload_ell(cgx_handle *h, int N, int nz, int maxNz,
       e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
-    cudaFree(tmp);
+    dev_free(h, tmp);
     CUDA_TRY(e);
   }
   h->N = N;
@@ -1395,7 +1457,7 @@ static cgx_status band_plan(cgx_handle *h, Band &B) {
   B = Band{};
   const int N = h->N;
   int *table = nullptr;
-  CUDA_TRY(cudaMalloc(&table, sizeof(int) * kBandTable));
+  CUDA_TRY(dev_alloc(h, (void **)&table, sizeof(int) * kBandTable));
   std::vector<int> host(kBandTable, kBandEmpty);
   int flag = 0;
   cudaError_t e = cudaMemcpyAsync(table, host.data(), sizeof(int) * kBandTable,
@@ -1413,7 +1475,7 @@ static cgx_status band_plan(cgx_handle *h, Band &B) {
     e = cudaMemcpyAsync(&flag, h->flag, sizeof(int), cudaMemcpyDeviceToHost,
                         h->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
-  cudaFree(table);
+  dev_free(h, table);
   CUDA_TRY(e);
   if (flag) return CGX_SUCCESS;
   std::vector<int> D;
@@ -1437,9 +1499,9 @@ static cgx_status band_fill(cgx_handle *h, Band &B) {
   const int N = h->N;
   B.ok = false;
   const size_t bytes = sizeof(float) * (size_t)N * kBandMaxK;
-  if (!B.U) CUDA_TRY(cudaMalloc(&B.U, bytes));
+  if (!B.U) CUDA_TRY(dev_alloc(h, (void **)&B.U, bytes));
   unsigned long long *counts = nullptr;
-  CUDA_TRY(cudaMalloc(&counts, 2 * sizeof(unsigned long long)));
+  CUDA_TRY(dev_alloc(h, (void **)&counts, 2 * sizeof(unsigned long long)));
   BandOffsets o{};
   o.K = B.K;
   for (int k = 0; k < B.K; k++) o.d[k] = B.d[k];
@@ -1465,7 +1527,7 @@ static cgx_status band_fill(cgx_handle *h, Band &B) {
     e = cudaMemcpyAsync(&flag, h->flag, sizeof(int), cudaMemcpyDeviceToHost,
                         h->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
-  cudaFree(counts);
+  dev_free(h, counts);
   CUDA_TRY(e);
   B.ok = flag == 0 && hc[0] == hc[1];
   return CGX_SUCCESS;
@@ -1484,7 +1546,7 @@ static cgx_status ensure_f32(cgx_handle *h) {
     size_t o_q = c.take<float>((size_t)N + kPad);
     size_t o_r64 = c.take<double>((size_t)N + kPad);
     size_t o_i16 = c.take<int16_t>((size_t)h->nz + kPad);
-    CUDA_TRY(cudaMalloc(&h->f32_mem, c.off));
+    CUDA_TRY(dev_alloc(h, (void **)&h->f32_mem, c.off));
     CUDA_TRY(cudaMemsetAsync(h->f32_mem, 0, c.off, h->stream));
     char *base = (char *)h->f32_mem;
     h->value32 = (float *)(base + o_v);
@@ -1512,7 +1574,7 @@ static cgx_status ensure_f32(cgx_handle *h) {
   }
   if (h->band.K > 0) {
     CGX_TRY(band_fill(h, h->band));
-    if (!h->band.ok) band_free(h->band);
+    if (!h->band.ok) band_free(h, h->band);
   }
   if (!h->band.ok && !h->sa_tried) {
     h->sa_tried = true;
@@ -1521,10 +1583,10 @@ static cgx_status ensure_f32(cgx_handle *h) {
     // to its longest one; A's FP32 CRS is faster there (measured on the 2M
     // point geometric graph: 64 against 71 us per product).
     if (h->sa.ok && 2 * h->sa.uniform < (long long)((h->N + 31) / 32))
-      sellu_free(h->sa);
+      sellu_free(h, h->sa);
   }
   if (h->sa.ok && !h->sa_val) {
-    CUDA_TRY(cudaMalloc(&h->sa_val, sizeof(float) * (h->sa.slots + kPad)));
+    CUDA_TRY(dev_alloc(h, (void **)&h->sa_val, sizeof(float) * (h->sa.slots + kPad)));
     CUDA_TRY(cudaMemsetAsync(h->sa_val, 0, sizeof(float) * (h->sa.slots + kPad),
                              h->stream));
   }
@@ -1850,7 +1912,7 @@ cgx_status learned_alloc(cgx_handle *h, int nnzL) {
   size_t o_o = take_n<float>(c, (size_t)N * NOUT);
   size_t o_y = take_n<float>(c, N), o_z = take_n<float>(c, N);
   size_t o_xb = take_n<double>(c, N);
-  CUDA_TRY(cudaMalloc(&L->mem, c.off));
+  CUDA_TRY(dev_alloc(h, (void **)&L->mem, c.off));
   CUDA_TRY(cudaMemsetAsync(L->mem, 0, c.off, h->stream));
   char *b = (char *)L->mem;
   L->dis = (double *)(b + o_dis);
@@ -1898,7 +1960,7 @@ cgx_status learned_train_alloc(cgx_handle *h) {
   size_t o_agg[3], o_pre[4];
   for (int q = 0; q < 3; q++) o_agg[q] = take_n<__nv_bfloat16>(c, (size_t)N * W);
   for (int q = 0; q < 4; q++) o_pre[q] = take_n<float>(c, (size_t)N * W);
-  CUDA_TRY(cudaMalloc(&L->train, c.off));
+  CUDA_TRY(dev_alloc(h, (void **)&L->train, c.off));
   CUDA_TRY(cudaMemsetAsync(L->train, 0, c.off, h->stream));
   char *b = (char *)L->train;
   k = 0;
@@ -1931,7 +1993,7 @@ cgx_status learned_train_alloc(cgx_handle *h) {
 // in int; the callers then keep their CRS kernels.
 cgx_status build_sellu(cgx_handle *h, const int *ptr, const int *col,
                        size_t nnz, SellU &S) {
-  sellu_free(S);
+  sellu_free(h, S);
   const int N = h->N;
   const int nsl = (N + 31) / 32;
   cudaStream_t s = h->stream;
@@ -1943,14 +2005,14 @@ cgx_status build_sellu(cgx_handle *h, const int *ptr, const int *col,
   size_t o_sm = take_n<int>(c, nsl / kScanBlock + 1);
   size_t o_tot = take_n<unsigned long long>(c, 4);
   void *tmp = nullptr;
-  CUDA_TRY(cudaMalloc(&tmp, c.off));
+  CUDA_TRY(dev_alloc(h, (void **)&tmp, c.off));
   char *t = (char *)tmp;
   int *wd = (int *)(t + o_wd);
   int *vc = (int *)(t + o_vc), *oc = (int *)(t + o_oc), *un = (int *)(t + o_un);
   int *vb = (int *)(t + o_vb), *ob = (int *)(t + o_ob), *sm = (int *)(t + o_sm);
   unsigned long long *tot = (unsigned long long *)(t + o_tot);
   auto fail_free = [&](cudaError_t e) {
-    cudaFree(tmp);
+    dev_free(h, tmp);
     return fail(CGX_ERROR_CUDA, cudaGetErrorString(e));
   };
   cudaError_t e = cudaMemsetAsync(tot, 0, 4 * sizeof(unsigned long long), s);
@@ -1964,7 +2026,7 @@ cgx_status build_sellu(cgx_handle *h, const int *ptr, const int *col,
     return fail_free(e);
   // Value slots: 128 per group.
   if (128 * ht[0] + 128 >= (unsigned long long)INT_MAX || ht[1] >= (unsigned long long)INT_MAX) {
-    cudaFree(tmp);
+    dev_free(h, tmp);
     return CGX_SUCCESS;
   }
   Carver d;
@@ -1972,7 +2034,7 @@ cgx_status build_sellu(cgx_handle *h, const int *ptr, const int *col,
   size_t o_map = take_n<int>(d, nnz);
   if ((e = scan(h, nsl, vc, vb, sm)) != cudaSuccess ||
       (e = scan(h, nsl, oc, ob, sm)) != cudaSuccess ||
-      (e = cudaMalloc(&S.mem, d.off)) != cudaSuccess ||
+      (e = dev_alloc(h, (void **)&S.mem, d.off)) != cudaSuccess ||
       (e = cudaMemsetAsync(S.mem, 0, d.off, s)) != cudaSuccess)
     return fail_free(e);
   char *b = (char *)S.mem;
@@ -1984,7 +2046,7 @@ cgx_status build_sellu(cgx_handle *h, const int *ptr, const int *col,
   if ((e = cudaGetLastError()) != cudaSuccess ||
       (e = cudaStreamSynchronize(s)) != cudaSuccess)
     return fail_free(e);
-  cudaFree(tmp);
+  dev_free(h, tmp);
   S.max_width = (int)ht[3];
   S.slots = 128 * (size_t)ht[0];
   S.uniform = (long long)ht[2];
@@ -1998,7 +2060,7 @@ cgx_status build_sell(cgx_handle *h) {
   Learned *L = h->L;
   L->sell_ok = false;
   L->gb_ok = false;
-  if (L->gb_mem) cudaFree(L->gb_mem);
+  if (L->gb_mem) dev_free(h, L->gb_mem);
   L->gb_mem = nullptr;
   // The band copy when A's offsets fit it.
   Band plan;
@@ -2008,7 +2070,7 @@ cgx_status build_sell(cgx_handle *h) {
     Carver c;
     size_t o_v = take_n<__nv_bfloat16>(c, (size_t)N * kBandMaxK);
     size_t o_m = take_n<int>(c, (size_t)L->nnzL);
-    CUDA_TRY(cudaMalloc(&L->gb_mem, c.off));
+    CUDA_TRY(dev_alloc(h, (void **)&L->gb_mem, c.off));
     L->gb_val = (__nv_bfloat16 *)((char *)L->gb_mem + o_v);
     L->g2b = (int *)((char *)L->gb_mem + o_m);
     BandOffsets o{};
@@ -2030,7 +2092,7 @@ cgx_status build_sell(cgx_handle *h) {
       L->gb_ok = true;
       return CGX_SUCCESS;
     }
-    cudaFree(L->gb_mem);
+    dev_free(h, L->gb_mem);
     L->gb_mem = nullptr;
   }
   CGX_TRY(build_sellu(h, L->gptr, L->gcol, (size_t)L->nnzL, L->sg));
@@ -2039,9 +2101,9 @@ cgx_status build_sell(cgx_handle *h) {
   Carver c;
   size_t o_g = take_n<__nv_bfloat16>(c, L->sg.slots);
   size_t o_t = take_n<__nv_bfloat16>(c, L->st.slots);
-  if (L->sell_val) cudaFree(L->sell_val);
+  if (L->sell_val) dev_free(h, L->sell_val);
   L->sell_val = nullptr;
-  CUDA_TRY(cudaMalloc(&L->sell_val, c.off));
+  CUDA_TRY(dev_alloc(h, (void **)&L->sell_val, c.off));
   CUDA_TRY(cudaMemsetAsync(L->sell_val, 0, c.off, h->stream));
   L->sg_val = (__nv_bfloat16 *)((char *)L->sell_val + o_g);
   L->st_val = (__nv_bfloat16 *)((char *)L->sell_val + o_t);
@@ -2237,7 +2299,7 @@ cgx_status cgx_learned_setup(cgx_handle *h) {
     size_t o_feat = c.take<float>((size_t)N * NIN + kPad);
     size_t o_nl = c.take<int>(N + kPad), o_nu = c.take<int>(N + kPad);
     size_t o_f = c.take<int>(4);
-    CUDA_TRY(cudaMalloc(&tmp, c.off));
+    CUDA_TRY(dev_alloc(h, (void **)&tmp, c.off));
     char *b = (char *)tmp;
     dis = (double *)(b + o_dis);
     ahat = (float *)(b + o_ahat);
@@ -2274,7 +2336,7 @@ cgx_status cgx_learned_setup(cgx_handle *h) {
     Carver c;
     size_t o_p = c.take<int>(N + 1 + kPad), o_s = c.take<int>(nb + kPad);
     void *t2 = nullptr;
-    CUDA_TRY(cudaMalloc(&t2, c.off));
+    CUDA_TRY(dev_alloc(h, (void **)&t2, c.off));
     tptr_tmp = (int *)((char *)t2 + o_p);
     sums_tmp = (int *)((char *)t2 + o_s);
     CUDA_TRY(scan(h, N, nlow, tptr_tmp, sums_tmp));
@@ -2287,15 +2349,15 @@ cgx_status cgx_learned_setup(cgx_handle *h) {
     int fl = 0;
     CUDA_TRY(cudaMemcpyAsync(&fl, flag, sizeof(int), cudaMemcpyDeviceToHost, s));
     CUDA_TRY(cudaStreamSynchronize(s));
-    cudaFree(t2);
+    dev_free(h, t2);
     if (fl) {
-      cudaFree(tmp);
+      dev_free(h, tmp);
       free_learned(h);
       return fail(CGX_ERROR_UNSUPPORTED,
                   "learned preconditioner: a diagonal entry is missing or not positive");
     }
     if (totals[0] != totals[1]) {
-      cudaFree(tmp);
+      dev_free(h, tmp);
       free_learned(h);
       return fail(CGX_ERROR_UNSUPPORTED,
                   "learned preconditioner: the matrix pattern is not symmetric");
@@ -2304,7 +2366,7 @@ cgx_status cgx_learned_setup(cgx_handle *h) {
   }
   cgx_status st = learned_alloc(h, L->nnzL);
   if (st != CGX_SUCCESS) {
-    cudaFree(tmp);
+    dev_free(h, tmp);
     free_learned(h);
     return st;
   }
@@ -2315,7 +2377,7 @@ cgx_status cgx_learned_setup(cgx_handle *h) {
   CUDA_TRY(cudaMemcpyAsync(L->nlow, nlow, sizeof(int) * N, cudaMemcpyDeviceToDevice, s));
   CUDA_TRY(cudaMemcpyAsync(L->nup, nup, sizeof(int) * N, cudaMemcpyDeviceToDevice, s));
   CUDA_TRY(cudaStreamSynchronize(s));
-  cudaFree(tmp);
+  dev_free(h, tmp);
   CUDA_TRY(scan(h, N, L->nlow, L->gptr, L->sums));
   CUDA_TRY(scan(h, N, L->nup, L->tptr, L->sums));
   k_fill_patterns<<<g, kThreads, 0, s>>>(N, h->ptr, h->index, L->gptr, L->tptr,
