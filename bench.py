@@ -476,7 +476,7 @@ def our_arm(args, world, rank, local):
         kk = kern[args.path]
         slots, uniform, slices = h.inner_layout()
         band = h.inner_band()
-        prof_name = "spmv_sellu_fp32_diffusion7_160.json"
+        prof_name = None  # ncu traffic is committed for the band form only
         if band:
             # Symmetric band: 4 FP32 values per row (diagonal and upper half;
             # the lower half is read from the rows above, in L1/L2), p once,
@@ -498,7 +498,7 @@ def our_arm(args, world, rank, local):
                 "peak": peak, "unit": "GB/s", "kernel": kname,
                 "algorithmic_bytes": fp32_spmv_bytes, "peak_kind": peak_kind}
         roof["frac"] = roof["achieved"] / peak
-        prof32 = read_traffic_profile(prof_name, args)
+        prof32 = read_traffic_profile(prof_name, args) if prof_name else None
         roof["traffic"] = prof32.get("dram_bytes_per_launch") if prof32 else None
 
     # End to end through the public C ABI: pinned host inputs uploaded every
