@@ -88,11 +88,21 @@ __device__ __forceinline__ bool grid_reduce(const double (&acc)[NACC],
   __syncthreads();
   if (!am_last) return false;
   __threadfence();
+  // All of a thread's partials are loaded before the first addition (one L2
+  // round trip instead of one per partial); they are added in the same order
+  // as a plain loop would, so the sums do not change.
+  constexpr int kPer = (kMaxGrid + kThreads - 1) / kThreads;
 #pragma unroll
   for (int a = 0; a < NACC; a++) {
+    double v[kPer];
+#pragma unroll
+    for (int k = 0; k < kPer; k++) {
+      const int b = threadIdx.x + k * kThreads;
+      v[k] = b < (int)gridDim.x ? __ldcg(&partials[a * kMaxGrid + b]) : 0.0;
+    }
     double s = 0.0;
-    for (int b = threadIdx.x; b < (int)gridDim.x; b += kThreads)
-      s += __ldcg(&partials[a * kMaxGrid + b]);
+#pragma unroll
+    for (int k = 0; k < kPer; k++) s += v[k];
     out[a] = block_sum(s, sh);
   }
   if (threadIdx.x == 0) *ticket = 0u;
