@@ -280,3 +280,58 @@ def test_time_spmv_measures_the_fused_product(handle):
     assert np.array_equal(handle.get_vector("X"), x1)
     with pytest.raises(cg.CgxError):
         handle.time_spmv(cg.PRECISION_FP64, reps=0)
+
+
+def test_reused_blocks_give_fresh_results():
+    """A handle keeps the device blocks of a replaced matrix and hands them
+    out again (uploads of the same size then allocate nothing). Whatever a
+    reused block held before must not reach a result: a sequence of uploads
+    of different sizes and formats, with the mixed and learned solves that
+    build further buffers, gives exactly what a fresh handle gives for each
+    matrix."""
+    mats = [G.diffusion3d(14, stencil=7, seed=11), random_crs(3001, max_len=12, seed=12, spd=True),
+            G.diffusion3d(14, stencil=7, seed=13), G.diffusion3d(9, stencil=27, seed=14)]
+
+    def run(h, A, fmt, precision):
+        b, _ = G.rhs_for(A, seed=A.N)
+        if fmt == "ELL":
+            m, length, index, data = G.to_ell(A)
+            h.upload_ell(A.N, A.nz, m, length, index, data)
+        else:
+            h.upload_crs(A.ptr, A.index, A.value)
+        h.upload_jacobi(1.0 / A.diagonal())
+        h.set_vector("K", b)
+        h.fill_vector("X", 0.0)
+        r = h.solve(max_iterations=5000, tolerance=1e-9, precision=precision)
+        return r["iterations"], h.get_vector("X")
+
+    plan = [(0, "CRS", cg.PRECISION_MIXED), (1, "CRS", cg.PRECISION_MIXED),
+            (2, "ELL", cg.PRECISION_FP64), (0, "CRS", cg.PRECISION_FP64),
+            (3, "CRS", cg.PRECISION_MIXED), (2, "CRS", cg.PRECISION_MIXED)]
+    from cgxx_b200 import learned as LRN
+
+    def run_learned(h, A):
+        b, _ = G.rhs_for(A, seed=A.N)
+        h.upload_crs(A.ptr, A.index, A.value)
+        h.upload_jacobi(1.0 / A.diagonal())
+        h.set_vector("K", b)
+        h.learned_setup()
+        net = cg.Gnn(0, LRN.init_params(0))
+        h.learned_factor(net, 1e-4)
+        net.close()
+        h.fill_vector("X", 0.0)
+        r = h.solve(max_iterations=5000, tolerance=1e-9, precision=cg.PRECISION_MIXED,
+                    preconditioner=cg.PRECOND_LEARNED)
+        return r["iterations"], h.get_vector("X")
+
+    with cg.Handle(0) as h:
+        for k, fmt, prec in plan:
+            it, x = run(h, mats[k], fmt, prec)
+            with cg.Handle(0) as fresh:
+                it0, x0 = run(fresh, mats[k], fmt, prec)
+            assert it == it0 and np.array_equal(x, x0), (k, fmt, prec)
+        for k in (0, 1, 0):
+            it, x = run_learned(h, mats[k])
+            with cg.Handle(0) as fresh:
+                it0, x0 = run_learned(fresh, mats[k])
+            assert it == it0 and np.array_equal(x, x0), ("learned", k)
