@@ -1162,6 +1162,12 @@ cgx_status cgx_upload_coo(cgx_handle *h, int N, int nz, const int *I,
                      CGX_FORMAT_COO, "COO");
 }
 
+// CRS and COO share the row-grouped device layout (ptr, index, value), which
+// the Jacobi set-up, the FP32 copies and the learned set-up read.
+static bool has_rows(const cgx_handle *h) {
+  return h->format == CGX_FORMAT_CRS || h->format == CGX_FORMAT_COO;
+}
+
 static cgx_status need_matrix(cgx_handle *h) {
   if (!h) return fail(CGX_ERROR_INVALID_ARGUMENT, "handle is NULL");
   if (h->format < 0)
@@ -1190,12 +1196,9 @@ cgx_status cgx_upload_jacobi(cgx_handle *h, const double *C) {
 cgx_status cgx_jacobi_from_matrix(cgx_handle *h) {
   CGX_TRY(need_matrix(h));
   DeviceGuard guard(h->device);
-  if (h->format != CGX_FORMAT_CRS) {
-    // ELL/COO: derive from the host-visible definition through a temporary
-    // CRS view is not available; compute on the device per format.
+  if (!has_rows(h))
     return fail(CGX_ERROR_UNSUPPORTED,
-                "cgx_jacobi_from_matrix supports CRS; upload C for ELL/COO");
-  }
+                "cgx_jacobi_from_matrix supports CRS and COO; upload C for ELL");
   k_jacobi_from_crs<<<grid_stream(h, h->N), kThreads, 0, h->stream>>>(
       h->N, h->ptr, h->index, h->value, h->C);
   CUDA_TRY(cudaGetLastError());
@@ -1695,8 +1698,8 @@ static cudaError_t launch_learned_iteration(cgx_handle *h,
 // the remaining steps use Jacobi (result.fell_back = 1).
 static cgx_status solve_mixed(cgx_handle *h, const cgx_options &o,
                               cgx_result &res) {
-  if (h->format != CGX_FORMAT_CRS)
-    return fail(CGX_ERROR_UNSUPPORTED, "mixed precision needs CRS");
+  if (!has_rows(h))
+    return fail(CGX_ERROR_UNSUPPORTED, "mixed precision needs CRS or COO");
   const bool want_learned = o.preconditioner == CGX_PRECONDITIONER_LEARNED;
   if (o.preconditioner != CGX_PRECONDITIONER_JACOBI && !want_learned)
     return fail(CGX_ERROR_UNSUPPORTED,
@@ -2274,8 +2277,8 @@ cgx_status cgx_update_crs_values(cgx_handle *h, const double *value) {
 
 cgx_status cgx_learned_setup(cgx_handle *h) {
   CGX_TRY(need_matrix(h));
-  if (h->format != CGX_FORMAT_CRS)
-    return fail(CGX_ERROR_UNSUPPORTED, "the learned preconditioner needs CRS");
+  if (!has_rows(h))
+    return fail(CGX_ERROR_UNSUPPORTED, "the learned preconditioner needs CRS or COO");
   DeviceGuard guard(h->device);
   cudaStream_t s = h->stream;
   const int N = h->N;
@@ -2633,8 +2636,8 @@ cgx_status cgx_solve(cgx_handle *h, const cgx_options *opts,
 cgx_status cgx_inner_matvec(cgx_handle *h, const float *x, float *y) {
   CGX_TRY(need_matrix(h));
   if (!x || !y) return fail(CGX_ERROR_INVALID_ARGUMENT, "x or y is NULL");
-  if (h->format != CGX_FORMAT_CRS)
-    return fail(CGX_ERROR_UNSUPPORTED, "the FP32 inner SpMV needs CRS");
+  if (!has_rows(h))
+    return fail(CGX_ERROR_UNSUPPORTED, "the FP32 inner SpMV needs CRS or COO");
   DeviceGuard guard(h->device);
   CGX_TRY(ensure_f32(h));
   CGX_TRY(pull_state(h));
@@ -2660,8 +2663,8 @@ cgx_status cgx_time_spmv(cgx_handle *h, cgx_precision precision, int reps,
     return fail(CGX_ERROR_INVALID_ARGUMENT, "unknown precision");
   DeviceGuard guard(h->device);
   if (precision == CGX_PRECISION_MIXED) {
-    if (h->format != CGX_FORMAT_CRS)
-      return fail(CGX_ERROR_UNSUPPORTED, "the FP32 inner SpMV needs CRS");
+    if (!has_rows(h))
+      return fail(CGX_ERROR_UNSUPPORTED, "the FP32 inner SpMV needs CRS or COO");
     CGX_TRY(ensure_f32(h));
   }
   // The products must not skip: clear the stop flags of the last solve.

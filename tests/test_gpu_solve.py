@@ -335,3 +335,41 @@ def test_reused_blocks_give_fresh_results():
             with cg.Handle(0) as fresh:
                 it0, x0 = run_learned(fresh, mats[k])
             assert it == it0 and np.array_equal(x, x0), ("learned", k)
+
+
+def test_mixed_and_learned_accept_coo():
+    """COO is held on the device in the row-grouped CRS layout, so the mixed
+    and learned paths and the device Jacobi set-up take it too. Uploaded as
+    the reference's reader produces it (lower triangle, then the mirrored
+    entries), the matrix solves as its CRS form does: the same iteration
+    counts and solutions within 1e-10 (only the order of entries inside a
+    row differs)."""
+    from cgxx_b200 import learned as LRN
+    A = G.diffusion3d(16, stencil=7, seed=21)
+    b, xs = G.rhs_for(A, seed=22)
+    I, J, V = G.symmetric_file_coo(A)
+    out = {}
+    for fmt in ("CRS", "COO"):
+        with cg.Handle(0) as h:
+            if fmt == "CRS":
+                h.upload_crs(A.ptr, A.index, A.value)
+            else:
+                h.upload_coo(A.N, I, J, V)
+            h.jacobi_from_matrix()
+            h.set_vector("K", b)
+            h.fill_vector("X", 0.0)
+            rm = h.solve(max_iterations=5000, tolerance=1e-9, precision=cg.PRECISION_MIXED)
+            xm = h.get_vector("X")
+            h.learned_setup()
+            net = cg.Gnn(0, LRN.init_params(0))
+            h.learned_factor(net, 1e-4)
+            net.close()
+            h.fill_vector("X", 0.0)
+            rl = h.solve(max_iterations=5000, tolerance=1e-9, precision=cg.PRECISION_MIXED,
+                         preconditioner=cg.PRECOND_LEARNED)
+            out[fmt] = (rm["iterations"], xm, rl["iterations"], h.get_vector("X"), h.inner_band())
+    (im, xm, il, xl, band), (im2, xm2, il2, xl2, band2) = out["CRS"], out["COO"]
+    assert band == band2 == [0, 1, 16, 256]
+    assert im == im2 and il == il2 and il < 0.75 * im
+    assert rel(xm2, xm) <= 1e-10 and rel(xl2, xl) <= 1e-10
+    assert rel(xm, xs) <= 1e-6 and rel(xl, xs) <= 1e-6
