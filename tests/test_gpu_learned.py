@@ -74,10 +74,11 @@ def test_factor_matches_oracle(name, make):
 
 @pytest.mark.parametrize("name,make", MATRICES + [
     ("diffusion7_13", lambda: G.diffusion3d(13, 7, sigma=1.0, corr_len=4.0, seed=5)),
-], ids=[m[0] for m in MATRICES] + ["diffusion7_13"])
+    ("poisson2d_37", lambda: G.poisson2d(37)),
+], ids=[m[0] for m in MATRICES] + ["diffusion7_13", "poisson2d_37"])
 def test_apply_matches_factor(name, make):
     """z = G (G^T r) + eps C r from the device (BF16 factor values, the band
-    copy of G for the 7-point stencils, SELL-U or FP32 CRS otherwise)
+    copy of G for the 7- and 5-point stencils, SELL-U or FP32 CRS otherwise)
     against the same product in FP64 from the factor the device reports:
     within 1.6e-2 of (|G| |G|^T |r|)_i + eps C_i |r_i| per row (two BF16
     roundings of the factor values, 2^-9 each, and FP32 sums)."""

@@ -171,16 +171,32 @@ def _asymmetric(A, rel=1e-4):
 
 
 # Inner SpMV form per case: the symmetric band for the 7-point stencil
-# (unsorted rows included), SELL-U for the 27-point stencil (14 stored
-# offsets) and for a 7-point stencil whose values are not exactly symmetric,
-# FP32 CRS for matrices whose slices would be mostly per-row.
+# (unsorted rows included), the 2D 5-point stencil and a tridiagonal matrix
+# (3 and 2 stored offsets: padding slots), SELL-U for the 27-point stencil
+# (14 stored offsets) and for a 7-point stencil whose values are not exactly
+# symmetric, FP32 CRS for matrices whose slices would be mostly per-row.
 _IRREGULAR = {
     "ragged": "crs",
     "unsorted": "band",
+    "poisson2d": "band",
+    "tridiagonal": "band",
     "wide": "crs",
     "stencil27_odd": "sellu",
     "stencil7_asym": "sellu",
 }
+
+
+def _tridiagonal(N, seed):
+    """SPD tridiagonal matrix with random couplings (offsets -1, 0, 1)."""
+    rng = np.random.default_rng(seed)
+    c = rng.uniform(0.5, 2.0, N - 1)
+    rows = np.concatenate([np.arange(N), np.arange(N - 1), np.arange(1, N)])
+    cols = np.concatenate([np.arange(N), np.arange(1, N), np.arange(N - 1)])
+    diag = np.zeros(N)
+    diag[:-1] += c
+    diag[1:] += c
+    vals = np.concatenate([diag + 0.01, -c, -c])
+    return G.crs_from_unsorted(N, rows, cols, vals)
 
 
 def _irregular_matrix(case):
@@ -192,15 +208,24 @@ def _irregular_matrix(case):
         return random_crs(777, max_len=80, seed=4, spd=True)
     if case == "stencil27_odd":
         return G.diffusion3d(11, stencil=27, seed=6)
+    if case == "poisson2d":
+        return G.poisson2d(37)
+    if case == "tridiagonal":
+        return _tridiagonal(1999, seed=8)
     return _asymmetric(G.diffusion3d(11, stencil=7, seed=6))
+
+
+def _expected_band(A):
+    """The offsets d >= 0 of A's entries (col - row), ascending."""
+    rows = np.repeat(np.arange(A.N), np.diff(A.ptr))
+    return sorted(set(int(d) for d in np.unique(A.index - rows) if d >= 0))
 
 
 def _check_inner_form(handle, A, form):
     slots, uniform, slices = handle.inner_layout()
     band = handle.inner_band()
     if form == "band":
-        n = round(A.N ** (1 / 3))
-        assert band == [0, 1, n, n * n] and slots == 0
+        assert band == _expected_band(A) and slots == 0
     elif form == "sellu":
         assert band == [] and slices == (A.N + 31) // 32 and uniform == slices
         assert slots >= A.nz
