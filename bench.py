@@ -412,10 +412,13 @@ def our_arm(args, world, rank, local):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1), r
 
-    def accuracy():
+    solutions = {args.path: x}
+
+    def accuracy(p):
         """FP64 true relative residual of the current X, and its relative
         error against the exact solution x* of b = A x* (FP64, on the CPU)."""
         xv = h.get_vector("X")
+        solutions[p] = xv
         return {"true_residual": float(np.linalg.norm(b - A.matvec(xv)) / np.linalg.norm(b)),
                 "rel_error_vs_exact": float(np.linalg.norm(xv - xs) / np.linalg.norm(xs))}
 
@@ -429,7 +432,12 @@ def our_arm(args, world, rank, local):
                    "iterations": runs[-1][1]["iterations"],
                    "outer_iterations": runs[-1][1]["outer_iterations"],
                    "fell_back": bool(runs[-1][1]["fell_back"])}
-        side[p].update(accuracy())
+        side[p].update(accuracy(p))
+    # Every path's error against the FP64 solve of the plain path (the
+    # reference's algorithm, bit-identical to its serial kernels).
+    xp = solutions["plain"]
+    for p, xv in solutions.items():
+        side[p]["rel_error_vs_fp64_solve"] = float(np.linalg.norm(xv - xp) / np.linalg.norm(xp))
     # Learned path: network set-up + inference alone.
     fe0 = torch.cuda.Event(enable_timing=True)
     fe1 = torch.cuda.Event(enable_timing=True)
@@ -570,6 +578,7 @@ def our_arm(args, world, rank, local):
             "speedup_vs_plain_fp64": side["plain"]["ms"] / ms,
             "kernel_us": kern,
             "plain_iteration_gbs": plain_iter_bytes / (plain_iter_us * 1e-6) / 1e9,
+            "plain_iteration_frac": plain_iter_bytes / (plain_iter_us * 1e-6) / 1e9 / peak,
             "roofline": roof,
             "roofline_fp64_spmv": fp64_roof,
             "clocks": clocks,
