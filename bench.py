@@ -213,16 +213,17 @@ def mtx_cache_path(A, name):
     return path
 
 
-def run_reference(A, b, name, reps, max_iter, tol, threads):
-    """Runs the reference's OpenMP CG in-process harness on the workload with
-    right-hand side b. Returns the list of per-repetition solve times (s) and
-    the iteration counts."""
+def run_reference(A, b, name, reps, max_iter, tol, threads, backend="omp"):
+    """Runs the reference's OpenMP (or serial) CG in-process harness on the
+    workload with right-hand side b. Returns the list of per-repetition solve
+    times (s) and the iteration counts."""
     from oracle import oracle as O
     path = mtx_cache_path(A, name)
     env = {"CG_MAX_ITER": str(max_iter), "CG_TOLERANCE": repr(tol),
-           "CG_MATRIX_FORMAT": "CRS", "CG_PRECONDITIONER": "jacobi",
-           "OMP_NUM_THREADS": str(threads), "OMP_PROC_BIND": "spread"}
-    summ, x = O.run_ref_harness(path, rhs=b, backend="omp", reps=reps, env=env)
+           "CG_MATRIX_FORMAT": "CRS", "CG_PRECONDITIONER": "jacobi"}
+    if backend == "omp":
+        env.update({"OMP_NUM_THREADS": str(threads), "OMP_PROC_BIND": "spread"})
+    summ, x = O.run_ref_harness(path, rhs=b, backend=backend, reps=reps, env=env)
     return summ["solve_time"], summ["iterations"], x
 
 
@@ -607,10 +608,26 @@ def cpu_baseline(A, b, args, full_iters):
     t = min(times)
     per_iter_ms = 1e3 * t / iters[-1]
     full = full_iters or iters[-1]
-    return {"value": per_iter_ms * full, "unit": "ms", "cores": threads, "kind": "reference",
-            "sample": f"{iters[-1]} iterations (CG_MAX_ITER={sample}) of the same solve by the "
-                      f"reference's CGOpenMP, best of 2, scaled to {full} iterations",
-            "ms_per_iteration": per_iter_ms}
+    out = {"value": per_iter_ms * full, "unit": "ms", "cores": threads, "kind": "reference",
+           "sample": f"{iters[-1]} iterations (CG_MAX_ITER={sample}) of the same solve by the "
+                     f"reference's CGOpenMP, best of 2, scaled to {full} iterations",
+           "ms_per_iteration": per_iter_ms}
+    # The reference's serial CG beside it, on one core: a smaller sample.
+    if O.ref_binary("ref_harness_serial") is not None:
+        ssample = 10
+        try:
+            st, si, _ = run_reference(A, b, workload_name(args), 1, ssample, args.tol, 1,
+                                      backend="serial")
+            s_ms = 1e3 * min(st) / si[-1]
+            out["serial"] = {"value": s_ms * full, "unit": "ms", "cores": 1,
+                             "kind": "reference",
+                             "sample": f"{si[-1]} iterations (CG_MAX_ITER={ssample}) of the same "
+                                       f"solve by the reference's serial CG, scaled to {full} "
+                                       "iterations",
+                             "ms_per_iteration": s_ms}
+        except Exception as e:  # pragma: no cover - reported, not fatal
+            out["serial"] = {"value": None, "error": str(e)[:200]}
+    return out
 
 
 def main():
