@@ -173,6 +173,7 @@ struct cgx_handle {
   int tile_cap = 0;
   int warp_cap = 0;  // k_crs_warp's tile capacity when 256-row tiles overflow
   int *ell_length = nullptr, *ell_index = nullptr;  // ELL
+  void *rows_mem = nullptr;  // ELL: the row layout (ptr, index, value), built on first use
   double *ell_data = nullptr;
   int ell_width = 0;
 
@@ -346,6 +347,8 @@ static void free_matrix(cgx_handle *h) {
   drop_graphs(h);
   free_learned(h);
   if (h->mat_mem) dev_free(h, h->mat_mem);
+  if (h->rows_mem) dev_free(h, h->rows_mem);
+  h->rows_mem = nullptr;
   if (h->vec_mem) dev_free(h, h->vec_mem);
   if (h->f32_mem) dev_free(h, h->f32_mem);
   h->mat_mem = h->vec_mem = h->f32_mem = nullptr;
@@ -408,6 +411,22 @@ __global__ void k_ell_tiles(int N, int width, const int *__restrict__ ci,
     const size_t o = ell_at(i, j, width);
     ti[o] = ci[e];
     td[o] = cd[e];
+  }
+}
+
+// Tile-major ELL to the row layout: row i's slots j < length[i] in order.
+__global__ void k_ell_to_rows(int N, int width, const int *__restrict__ length,
+                              const int *__restrict__ eidx,
+                              const double *__restrict__ edat,
+                              const int *__restrict__ ptr, int *__restrict__ index,
+                              double *__restrict__ value) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N;
+       i += gridDim.x * blockDim.x) {
+    const int len = length[i], o = ptr[i];
+    for (int j = 0; j < len; j++) {
+      index[o + j] = eidx[ell_at(i, j, width)];
+      value[o + j] = edat[ell_at(i, j, width)];
+    }
   }
 }
 
@@ -1001,6 +1020,25 @@ static cgx_status check_flag(cgx_handle *h, const char *what) {
 
 extern "C" {
 
+// Tile capacity of the staged CRS SpMV: the largest nonzero count of a
+// 256-row tile, bounded so that two stages fit next to each other with
+// several CTAs per SM; larger tiles fall back to direct loads. Rows too long
+// for those tiles: 32-row tiles staged per warp (k_crs_warp) when they hold
+// at most 2048 nonzeros.
+static void set_tile_caps(cgx_handle *h, const int *ptr, int N) {
+  int maxTile = 0;
+  for (int r0 = 0; r0 < N; r0 += kThreads)
+    maxTile = std::max(maxTile, ptr[std::min(N, r0 + kThreads)] - ptr[r0]);
+  h->tile_cap = std::min(maxTile, 4096);
+  h->warp_cap = 0;
+  if (maxTile > 4096) {
+    int maxWarp = 0;
+    for (int r0 = 0; r0 < N; r0 += 32)
+      maxWarp = std::max(maxWarp, ptr[std::min(N, r0 + 32)] - ptr[r0]);
+    if (maxWarp <= 2048) h->warp_cap = maxWarp;
+  }
+}
+
 // Row-grouped device layout shared by CRS and COO: row pointers, column
 // indices and values in storage order, validated on the device.
 static cgx_status upload_rows(cgx_handle *h, int N, int nz, const int *ptr,
@@ -1009,24 +1047,7 @@ static cgx_status upload_rows(cgx_handle *h, int N, int nz, const int *ptr,
   DeviceGuard guard(h->device);
   CUDA_TRY(cudaStreamSynchronize(h->stream));
   free_matrix(h);
-  // Tile capacity of the staged SpMV: the largest nonzero count of a
-  // 256-row tile, bounded so that two stages fit next to each other with
-  // several CTAs per SM; larger tiles fall back to direct loads.
-  int maxTile = 0;
-  for (int r0 = 0; r0 < N; r0 += kThreads) {
-    int r1 = std::min(N, r0 + kThreads);
-    maxTile = std::max(maxTile, ptr[r1] - ptr[r0]);
-  }
-  h->tile_cap = std::min(maxTile, 4096);
-  // Rows too long for those tiles: 32-row tiles staged per warp (k_crs_warp)
-  // when they hold at most 2048 nonzeros.
-  h->warp_cap = 0;
-  if (maxTile > 4096) {
-    int maxWarp = 0;
-    for (int r0 = 0; r0 < N; r0 += 32)
-      maxWarp = std::max(maxWarp, ptr[std::min(N, r0 + 32)] - ptr[r0]);
-    if (maxWarp <= 2048) h->warp_cap = maxWarp;
-  }
+  set_tile_caps(h, ptr, N);
 
   Carver c;
   size_t o_ptr = c.take<int>((size_t)N + 1 + kPad);
@@ -1162,11 +1183,10 @@ cgx_status cgx_upload_coo(cgx_handle *h, int N, int nz, const int *I,
                      CGX_FORMAT_COO, "COO");
 }
 
-// CRS and COO share the row-grouped device layout (ptr, index, value), which
-// the Jacobi set-up, the FP32 copies and the learned set-up read.
-static bool has_rows(const cgx_handle *h) {
-  return h->format == CGX_FORMAT_CRS || h->format == CGX_FORMAT_COO;
-}
+// The row layout (ptr, index, value) that the Jacobi set-up, the FP32 copies
+// and the learned set-up read: CRS and COO hold it from the upload; for ELL
+// it is built on first use (ensure_rows).
+static cgx_status ensure_rows(cgx_handle *h);
 
 static cgx_status need_matrix(cgx_handle *h) {
   if (!h) return fail(CGX_ERROR_INVALID_ARGUMENT, "handle is NULL");
@@ -1196,9 +1216,7 @@ cgx_status cgx_upload_jacobi(cgx_handle *h, const double *C) {
 cgx_status cgx_jacobi_from_matrix(cgx_handle *h) {
   CGX_TRY(need_matrix(h));
   DeviceGuard guard(h->device);
-  if (!has_rows(h))
-    return fail(CGX_ERROR_UNSUPPORTED,
-                "cgx_jacobi_from_matrix supports CRS and COO; upload C for ELL");
+  CGX_TRY(ensure_rows(h));
   k_jacobi_from_crs<<<grid_stream(h, h->N), kThreads, 0, h->stream>>>(
       h->N, h->ptr, h->index, h->value, h->C);
   CUDA_TRY(cudaGetLastError());
@@ -1698,8 +1716,7 @@ static cudaError_t launch_learned_iteration(cgx_handle *h,
 // the remaining steps use Jacobi (result.fell_back = 1).
 static cgx_status solve_mixed(cgx_handle *h, const cgx_options &o,
                               cgx_result &res) {
-  if (!has_rows(h))
-    return fail(CGX_ERROR_UNSUPPORTED, "mixed precision needs CRS or COO");
+  CGX_TRY(ensure_rows(h));
   const bool want_learned = o.preconditioner == CGX_PRECONDITIONER_LEARNED;
   if (o.preconditioner != CGX_PRECONDITIONER_JACOBI && !want_learned)
     return fail(CGX_ERROR_UNSUPPORTED,
@@ -2200,6 +2217,57 @@ cudaError_t gnn_backward(cgx_handle *h, const float *P) {
 
 }  // namespace
 
+static cgx_status ensure_rows(cgx_handle *h) {
+  if (h->format == CGX_FORMAT_CRS || h->format == CGX_FORMAT_COO) return CGX_SUCCESS;
+  if (h->format != CGX_FORMAT_ELL)
+    return fail(CGX_ERROR_INVALID_STATE, "no matrix has been uploaded");
+  if (h->rows_mem) return CGX_SUCCESS;
+  // Row i's slots j < length[i] in slot order (the reference's ELL keeps a
+  // row's CRS order in its slots, Matrix.cpp:339-361). The row pointers come
+  // first: the total sizes the index and value arrays.
+  const int N = h->N;
+  const int nb = (N + cgx::learned::kScanBlock - 1) / cgx::learned::kScanBlock;
+  Carver c;
+  const size_t o_ptr = c.take<int>((size_t)N + 1 + kPad), o_sums = c.take<int>((size_t)nb);
+  void *pmem = nullptr;
+  CUDA_TRY(dev_alloc(h, &pmem, c.off));
+  int *ptr = (int *)((char *)pmem + o_ptr);
+  std::vector<int> hptr((size_t)N + 1);
+  cudaError_t e = scan(h, N, h->ell_length, ptr, (int *)((char *)pmem + o_sums));
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(hptr.data(), ptr, sizeof(int) * ((size_t)N + 1),
+                        cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) {
+    dev_free(h, pmem);
+    CUDA_TRY(e);
+  }
+  const size_t nz = (size_t)hptr[N];
+  Carver d;
+  const size_t q_ptr = d.take<int>((size_t)N + 1 + kPad), q_idx = d.take<int>(nz + kPad);
+  const size_t q_val = d.take<double>(nz + kPad);
+  e = dev_alloc(h, &h->rows_mem, d.off);
+  if (e == cudaSuccess) e = cudaMemsetAsync(h->rows_mem, 0, d.off, h->stream);
+  char *base = (char *)h->rows_mem;
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(base + q_ptr, ptr, sizeof(int) * ((size_t)N + 1),
+                        cudaMemcpyDeviceToDevice, h->stream);
+  if (e == cudaSuccess) {
+    k_ell_to_rows<<<grid_stream(h, N), kThreads, 0, h->stream>>>(
+        N, h->ell_width, h->ell_length, h->ell_index, h->ell_data,
+        (const int *)(base + q_ptr), (int *)(base + q_idx), (double *)(base + q_val));
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  dev_free(h, pmem);
+  CUDA_TRY(e);
+  h->ptr = (int *)(base + q_ptr);
+  h->index = (int *)(base + q_idx);
+  h->value = (double *)(base + q_val);
+  set_tile_caps(h, hptr.data(), N);
+  return CGX_SUCCESS;
+}
+
 extern "C" {
 
 int cgx_gnn_param_count(void) { return NPARAMS; }
@@ -2277,9 +2345,8 @@ cgx_status cgx_update_crs_values(cgx_handle *h, const double *value) {
 
 cgx_status cgx_learned_setup(cgx_handle *h) {
   CGX_TRY(need_matrix(h));
-  if (!has_rows(h))
-    return fail(CGX_ERROR_UNSUPPORTED, "the learned preconditioner needs CRS or COO");
   DeviceGuard guard(h->device);
+  CGX_TRY(ensure_rows(h));
   cudaStream_t s = h->stream;
   const int N = h->N;
   const bool fresh = !h->L;
@@ -2636,9 +2703,8 @@ cgx_status cgx_solve(cgx_handle *h, const cgx_options *opts,
 cgx_status cgx_inner_matvec(cgx_handle *h, const float *x, float *y) {
   CGX_TRY(need_matrix(h));
   if (!x || !y) return fail(CGX_ERROR_INVALID_ARGUMENT, "x or y is NULL");
-  if (!has_rows(h))
-    return fail(CGX_ERROR_UNSUPPORTED, "the FP32 inner SpMV needs CRS or COO");
   DeviceGuard guard(h->device);
+  CGX_TRY(ensure_rows(h));
   CGX_TRY(ensure_f32(h));
   CGX_TRY(pull_state(h));
   h->host_st->in_stop = 0;
@@ -2663,8 +2729,7 @@ cgx_status cgx_time_spmv(cgx_handle *h, cgx_precision precision, int reps,
     return fail(CGX_ERROR_INVALID_ARGUMENT, "unknown precision");
   DeviceGuard guard(h->device);
   if (precision == CGX_PRECISION_MIXED) {
-    if (!has_rows(h))
-      return fail(CGX_ERROR_UNSUPPORTED, "the FP32 inner SpMV needs CRS or COO");
+    CGX_TRY(ensure_rows(h));
     CGX_TRY(ensure_f32(h));
   }
   // The products must not skip: clear the stop flags of the last solve.

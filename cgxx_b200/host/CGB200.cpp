@@ -8,7 +8,7 @@
 // Additional environment switches (all optional):
 //   CG_B200_FUSED      1 (default) fused device solve, 0 per-kernel calls
 //   CG_B200_PRECISION  fp64 (default) | mixed  (FP32 inner + FP64 refinement,
-//                      CRS or COO, Jacobi)
+//                      Jacobi)
 //   CG_B200_LOOP       graph (default) | chunked | kernels (per-kernel
 //                      device times in the summary)
 //   CG_B200_DEVICE     CUDA device ordinal (default 0)
@@ -165,9 +165,8 @@ public:
       else
         badEnv("CG_B200_PRECISION", "fp64, or mixed");
       if (precision == CGX_PRECISION_MIXED &&
-          (matrixFormat == MatrixFormatELL ||
-           preconditioner != PreconditionerJacobi)) {
-        std::cerr << "Mixed precision needs CRS or COO and Jacobi!" << std::endl;
+          preconditioner != PreconditionerJacobi) {
+        std::cerr << "Mixed precision needs Jacobi!" << std::endl;
         std::exit(1);
       }
     }

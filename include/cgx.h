@@ -73,7 +73,7 @@ typedef enum cgx_preconditioner {
 
 typedef enum cgx_precision {
   CGX_PRECISION_FP64 = 0, /* the reference's arithmetic (def.h:6) */
-  CGX_PRECISION_MIXED = 1 /* FP32 inner PCG inside FP64 refinement (CRS, COO) */
+  CGX_PRECISION_MIXED = 1 /* FP32 inner PCG inside FP64 refinement */
 } cgx_precision;
 
 typedef enum cgx_loop {
@@ -139,7 +139,9 @@ cgx_status cgx_synchronize(cgx_handle *h);
 cgx_status cgx_upload_crs(cgx_handle *h, int N, int nz, const int *ptr,
                           const int *index, const double *value);
 /* ELL as in MatrixDataELL (Matrix.h:74-87): column-major, element (i, j) at
- * j*N + i, length[i] entries used per row, maxNz slots per row. */
+ * j*N + i, length[i] entries used per row, maxNz slots per row. The paths
+ * that read rows (mixed, learned, cgx_jacobi_from_matrix) build a CRS copy
+ * of it on the device on first use. */
 cgx_status cgx_upload_ell(cgx_handle *h, int N, int nz, int maxNz,
                           const int *length, const int *index,
                           const double *data);
@@ -152,8 +154,7 @@ cgx_status cgx_upload_coo(cgx_handle *h, int N, int nz, const int *I,
 cgx_status cgx_upload_jacobi(cgx_handle *h, const double *C);
 /* Computes C[i] = 1 / A_ii on the device from the uploaded matrix, with the
  * semantics of Jacobi::init (Preconditioner.cpp:13-23): the last diagonal
- * entry of a row in file order wins; a row without one gets C = 0. CRS and
- * COO. */
+ * entry of a row in file order wins; a row without one gets C = 0. */
 cgx_status cgx_jacobi_from_matrix(cgx_handle *h);
 cgx_status cgx_set_vector(cgx_handle *h, cgx_vector v, const double *host);
 /* CGCUDA::doTransferFrom (cuda/CGCUDA.cu:77-112) for one vector. */
@@ -198,8 +199,8 @@ cgx_status cgx_gnn_get_params(cgx_gnn *g, float *params);
 /* Replaces the values of the uploaded CRS matrix (same pattern); `value`
  * may be host or device memory. */
 cgx_status cgx_update_crs_values(cgx_handle *h, const double *value);
-/* Builds the Jacobi-scaled graph of the uploaded CRS or COO matrix (needs
- * positive diagonal entries and a structurally symmetric pattern). After
+/* Builds the Jacobi-scaled graph of the uploaded matrix (needs positive
+ * diagonal entries and a structurally symmetric pattern). After
  * cgx_update_crs_values it only recomputes the scaled values. */
 cgx_status cgx_learned_setup(cgx_handle *h);
 /* Network inference: G and G^T for the current matrix, eps >= 0. */
@@ -270,7 +271,7 @@ cgx_status cgx_inner_band(cgx_handle *h, int *stored_offsets, int *offsets);
 /* y = A x by the inner FP32 SpMV of the mixed and learned paths, on
  * whichever form it uses (no counterpart in the reference; it exposes that
  * product to tests): x and y are N host floats. Builds the FP32 copy if
- * needed; overwrites the inner p and q and the solver scalars. CRS or COO. */
+ * needed; overwrites the inner p and q and the solver scalars. */
 cgx_status cgx_inner_matvec(cgx_handle *h, const float *x, float *y);
 
 /* Layout of A's FP32 copy used by the inner SpMV of the mixed and learned

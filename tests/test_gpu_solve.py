@@ -362,24 +362,27 @@ def test_reused_blocks_give_fresh_results():
             assert it == it0 and np.array_equal(x, x0), ("learned", k)
 
 
-def test_mixed_and_learned_accept_coo():
-    """COO is held on the device in the row-grouped CRS layout, so the mixed
-    and learned paths and the device Jacobi set-up take it too. Uploaded as
-    the reference's reader produces it (lower triangle, then the mirrored
-    entries), the matrix solves as its CRS form does: the same iteration
-    counts and solutions within 1e-10 (only the order of entries inside a
-    row differs)."""
+def test_mixed_and_learned_accept_every_format():
+    """The mixed and learned paths and the device Jacobi set-up read the row
+    layout: COO holds it from the upload (grouped by row), ELL builds it on
+    first use. The COO form as the reference's reader produces it (lower
+    triangle, then the mirrored entries) and the ELL form solve as the CRS
+    form does: the same iteration counts and solutions within 1e-10 (only
+    the order of entries inside a row may differ)."""
     from cgxx_b200 import learned as LRN
     A = G.diffusion3d(16, stencil=7, seed=21)
     b, xs = G.rhs_for(A, seed=22)
     I, J, V = G.symmetric_file_coo(A)
     out = {}
-    for fmt in ("CRS", "COO"):
+    for fmt in ("CRS", "COO", "ELL"):
         with cg.Handle(0) as h:
             if fmt == "CRS":
                 h.upload_crs(A.ptr, A.index, A.value)
-            else:
+            elif fmt == "COO":
                 h.upload_coo(A.N, I, J, V)
+            else:
+                m, length, index, data = G.to_ell(A)
+                h.upload_ell(A.N, A.nz, m, length, index, data)
             h.jacobi_from_matrix()
             h.set_vector("K", b)
             h.fill_vector("X", 0.0)
@@ -393,8 +396,10 @@ def test_mixed_and_learned_accept_coo():
             rl = h.solve(max_iterations=5000, tolerance=1e-9, precision=cg.PRECISION_MIXED,
                          preconditioner=cg.PRECOND_LEARNED)
             out[fmt] = (rm["iterations"], xm, rl["iterations"], h.get_vector("X"), h.inner_band())
-    (im, xm, il, xl, band), (im2, xm2, il2, xl2, band2) = out["CRS"], out["COO"]
-    assert band == band2 == [0, 1, 16, 256]
-    assert im == im2 and il == il2 and il < 0.75 * im
-    assert rel(xm2, xm) <= 1e-10 and rel(xl2, xl) <= 1e-10
+    im, xm, il, xl, band = out["CRS"]
+    assert band == [0, 1, 16, 256] and il < 0.75 * im
     assert rel(xm, xs) <= 1e-6 and rel(xl, xs) <= 1e-6
+    for fmt in ("COO", "ELL"):
+        im2, xm2, il2, xl2, band2 = out[fmt]
+        assert band2 == band and im2 == im and il2 == il, fmt
+        assert rel(xm2, xm) <= 1e-10 and rel(xl2, xl) <= 1e-10, fmt

@@ -43,8 +43,8 @@ def test_new_switch_errors():
     assert p.returncode == 1 and "CG_B200_PRECISION" in p.stderr
     p = run([mtx], {"CG_B200_LOOP": "spin"})
     assert p.returncode == 1 and "CG_B200_LOOP" in p.stderr
-    p = run([mtx], {"CG_B200_PRECISION": "mixed", "CG_MATRIX_FORMAT": "ELL"})
-    assert p.returncode == 1 and "Mixed precision needs CRS" in p.stderr
+    p = run([mtx], {"CG_B200_PRECISION": "mixed", "CG_PRECONDITIONER": "none"})
+    assert p.returncode == 1 and "Mixed precision needs Jacobi" in p.stderr
 
 
 def test_reads_matrix_before_touching_the_device():
