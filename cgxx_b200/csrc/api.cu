@@ -2478,6 +2478,9 @@ cgx_status cgx_learned_factor(cgx_handle *h, cgx_gnn *gn, double eps) {
   if (!(eps >= 0)) return fail(CGX_ERROR_INVALID_ARGUMENT, "eps must be >= 0");
   DeviceGuard guard(h->device);
   CUDA_TRY(gnn_forward(h, gn->params, true));
+  // eps is a kernel argument of the captured inner-solve graphs: a new value
+  // needs new graphs (the factor's values are in device memory and need none).
+  if (h->L->eps != (float)eps) drop_graphs(h);
   h->L->eps = (float)eps;
   h->L->has_factor = true;
   return CGX_SUCCESS;

@@ -319,3 +319,32 @@ def test_learned_setup_rejects_unsymmetric_pattern():
         h.learned_setup()
     assert "symmetric" in e.value.message
     h.close()
+
+
+def test_eps_change_reaches_the_solve():
+    """eps is an argument of the kernels that the cached inner-solve graph
+    holds; a new eps must reach the next solve. The solve after
+    learned_factor(eps2) equals a fresh handle's solve with eps2, and differs
+    from the one with eps1 (eps2 large enough to change the iterates)."""
+    A = G.diffusion3d(14, 7, sigma=1.0, corr_len=4.0, seed=9)
+    b, _ = G.rhs_for(A, seed=10)
+    net = cg.Gnn(0, GO.init_params(0))
+
+    def solve(h, eps):
+        h.learned_factor(net, eps)
+        h.set_vector("K", b)
+        h.fill_vector("X", 0.0)
+        r = h.solve(max_iterations=5000, tolerance=1e-9, precision=cg.PRECISION_MIXED,
+                    preconditioner=cg.PRECOND_LEARNED)
+        return r["iterations"], h.get_vector("X")
+
+    h = _setup(A)
+    it1, x1 = solve(h, 1e-4)
+    it2, x2 = solve(h, 1.0)
+    h.close()
+    fresh = _setup(A)
+    it2f, x2f = solve(fresh, 1.0)
+    fresh.close()
+    net.close()
+    assert it2 == it2f and np.array_equal(x2, x2f)
+    assert it1 != it2 or not np.array_equal(x1, x2)
