@@ -12,10 +12,21 @@
 //   CG_B200_LOOP       graph (default) | chunked | kernels (per-kernel
 //                      device times in the summary)
 //   CG_B200_DEVICE     CUDA device ordinal (default 0)
+//   CG_B200_LEARNED    a weight file of the learned preconditioner (e.g.
+//                      cgxx_b200/weights/diffusion7.gnn): M^-1 = G G^T + eps C
+//                      with G from the network, inside the mixed-precision
+//                      solve (implies CG_B200_PRECISION=mixed; needs Jacobi,
+//                      which is also the fallback, and the fused solve). The
+//                      factor is built once per upload, like Jacobi::init,
+//                      and its time is printed in the summary.
+#include <chrono>
+#include <cstdint>
 #include <cstdlib>
 #include <cstring>
+#include <fstream>
 #include <iostream>
 #include <string>
+#include <vector>
 
 #include "CG.h"
 #include "cgx.h"
@@ -37,6 +48,36 @@ void ok(cgx_status s) {
   std::exit(1);
 }
 
+// Parameters of a weight file written by cgxx_b200/learned.py: the magic
+// "CGXGNN01", a little-endian uint32 header length, a JSON header (not
+// needed here) and cgx_gnn_param_count() little-endian floats.
+std::vector<float> readWeights(const std::string &path) {
+  std::ifstream f(path, std::ios::binary);
+  if (!f) {
+    std::cerr << "Could not open weight file " << path << "!" << std::endl;
+    std::exit(1);
+  }
+  char magic[8];
+  std::uint32_t len = 0;
+  const int n = cgx_gnn_param_count();
+  std::vector<float> params((size_t)n);
+  bool good = (bool)f.read(magic, 8) && std::memcmp(magic, "CGXGNN01", 8) == 0 &&
+              (bool)f.read(reinterpret_cast<char *>(&len), 4) &&
+              (bool)f.seekg(len, std::ios::cur) &&
+              (bool)f.read(reinterpret_cast<char *>(params.data()),
+                           (std::streamsize)(sizeof(float) * params.size()));
+  if (good) {
+    f.peek();
+    good = f.eof();  // nothing after the parameters
+  }
+  if (!good) {
+    std::cerr << "Invalid weight file " << path << "! (expected " << n
+              << " parameters)" << std::endl;
+    std::exit(1);
+  }
+  return params;
+}
+
 }  // namespace
 
 class CGB200 : public CG {
@@ -47,6 +88,12 @@ class CGB200 : public CG {
   int loop = CGX_LOOP_GRAPH;
   int device = 0;
   cgx_result last{};
+  // Learned preconditioner (CG_B200_LEARNED).
+  std::string learnedFile;
+  std::vector<float> learnedParams;
+  cgx_gnn *gnn = nullptr;
+  double learnedSetupSeconds = 0;
+  static constexpr double kLearnedEps = 1e-4;
 
   static cgx_vector vec(Vector v) { return (cgx_vector)v; }
 
@@ -91,6 +138,16 @@ class CGB200 : public CG {
       if (preconditioner == PreconditionerJacobi)
         ok(cgx_upload_jacobi(h, jacobi->C));
       ok(cgx_set_vector(h, CGX_VECTOR_K, k));
+      if (gnn) {
+        // The learned factor for this matrix: scaled graph and inference.
+        const auto t0 = std::chrono::steady_clock::now();
+        ok(cgx_learned_setup(h));
+        ok(cgx_learned_factor(h, gnn, kLearnedEps));
+        ok(cgx_synchronize(h));
+        learnedSetupSeconds = std::chrono::duration<double>(
+                                  std::chrono::steady_clock::now() - t0)
+                                  .count();
+      }
       uploaded = true;
     }
     ok(cgx_set_vector(h, CGX_VECTOR_X, x));
@@ -130,9 +187,10 @@ class CGB200 : public CG {
     ok(cgx_default_options(&o));
     o.max_iterations = maxIterations;
     o.tolerance = tolerance;
-    o.preconditioner = preconditioner == PreconditionerJacobi
-                           ? CGX_PRECONDITIONER_JACOBI
-                           : CGX_PRECONDITIONER_NONE;
+    o.preconditioner = gnn ? CGX_PRECONDITIONER_LEARNED
+                           : preconditioner == PreconditionerJacobi
+                               ? CGX_PRECONDITIONER_JACOBI
+                               : CGX_PRECONDITIONER_NONE;
     o.precision = precision;
     o.loop = loop;
     ok(cgx_solve(h, &o, &last));
@@ -187,6 +245,22 @@ public:
       if (*end != 0 || d < 0) badEnv("CG_B200_DEVICE", "a device ordinal");
       device = (int)d;
     }
+    if (const char *v = std::getenv("CG_B200_LEARNED"); v && *v) {
+      const char *pv = std::getenv("CG_B200_PRECISION");
+      if (pv && *pv && std::string(pv) != "mixed") {
+        std::cerr << "The learned preconditioner runs in mixed precision!"
+                  << std::endl;
+        std::exit(1);
+      }
+      if (preconditioner != PreconditionerJacobi || !fused) {
+        std::cerr << "The learned preconditioner needs Jacobi and the fused solve!"
+                  << std::endl;
+        std::exit(1);
+      }
+      learnedFile = v;
+      learnedParams = readWeights(learnedFile);
+      precision = CGX_PRECISION_MIXED;
+    }
   }
 
   // The matrix is read first so that file errors are reported before any
@@ -194,6 +268,7 @@ public:
   void init(const char *matrixFile) override {
     CG::init(matrixFile);
     ok(cgx_create(&h, device));
+    if (!learnedParams.empty()) ok(cgx_gnn_create(&gnn, device, learnedParams.data()));
   }
 
   void printSummary() override {
@@ -206,6 +281,11 @@ public:
                                     : "FP64");
       if (precision == CGX_PRECISION_MIXED)
         printPadded("Refinement steps:", std::to_string(last.outer_iterations));
+      if (gnn) {
+        printPadded("Learned factor:", learnedFile);
+        printPadded("Learned set-up time:", std::to_string(learnedSetupSeconds));
+        printPadded("Fell back to Jacobi:", last.fell_back ? "yes" : "no");
+      }
       static const char *loops[] = {"CUDA graph (while node)",
                                     "CUDA graph chunks", "kernel launches"};
       printPadded("Device loop:", loops[loop]);
@@ -214,6 +294,8 @@ public:
 
   void cleanup() override {
     CG::cleanup();
+    if (gnn) cgx_gnn_destroy(gnn);
+    gnn = nullptr;
     if (h) cgx_destroy(h);
     h = nullptr;
   }

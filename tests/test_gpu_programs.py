@@ -89,3 +89,22 @@ def test_cg_b200_mixed_precision():
 def test_reference_solve_drives_device_kernels(case):
     env = {"CG_MATRIX_FORMAT": case["format"], "CG_PRECONDITIONER": case["preconditioner"]}
     check(run(ADAPTER, os.path.join(GOLD, case["matrix"]), env), case)
+
+
+def test_cg_b200_learned_preconditioner(tmp_path):
+    """CG_B200_LEARNED: the program solves with M^-1 = G G^T + eps C from the
+    shipped weights inside the mixed-precision solve, passes the reference's
+    check of x = 1, and needs fewer than 3/4 of the inner iterations of the
+    Jacobi mixed run on the same file."""
+    from cgxx_b200 import generators as G
+    A = G.diffusion3d(20, stencil=7, sigma=1.0, corr_len=4.0, seed=5)
+    mtx = str(tmp_path / "d20.mtx")
+    G.write_mtx_symmetric_py(mtx, A)
+    weights = os.path.join(REPO, "cgxx_b200", "weights", "diffusion7.gnn")
+    out_l = run(EXE, mtx, {"CG_B200_LEARNED": weights})
+    out_j = run(EXE, mtx, {"CG_B200_PRECISION": "mixed"})
+    s_l, s_j = O.parse_summary(out_l), O.parse_summary(out_j)
+    assert s_l["correct"] and s_j["correct"]
+    assert s_l["residual"][0] <= 1e-9
+    assert "Fell back to Jacobi:" in out_l and re.search(r"Fell back to Jacobi:\s+no", out_l)
+    assert s_l["iterations"][0] < 0.75 * s_j["iterations"][0], (s_l["iterations"], s_j["iterations"])

@@ -54,3 +54,24 @@ def test_reads_matrix_before_touching_the_device():
     assert p.returncode == 1
     assert p.stderr.strip() == "Can't open file with matrix!"
     assert p.stdout.startswith("Reading matrix from")
+
+
+def test_learned_switch_errors(tmp_path):
+    """CG_B200_LEARNED names a weight file of the learned preconditioner; a
+    missing or malformed file and the combinations the learned path cannot
+    run are reported before any device work."""
+    mtx = os.path.join(GOLD, "poisson16.mtx")
+    weights = os.path.join(REPO, "cgxx_b200", "weights", "diffusion7.gnn")
+    p = run([mtx], {"CG_B200_LEARNED": str(tmp_path / "missing.gnn")})
+    assert p.returncode == 1 and "Could not open weight file" in p.stderr
+    bad = tmp_path / "bad.gnn"
+    bad.write_bytes(open(weights, "rb").read()[:-4])  # one parameter short
+    p = run([mtx], {"CG_B200_LEARNED": str(bad)})
+    assert p.returncode == 1 and "Invalid weight file" in p.stderr
+    p = run([mtx], {"CG_B200_LEARNED": mtx})
+    assert p.returncode == 1 and "Invalid weight file" in p.stderr
+    p = run([mtx], {"CG_B200_LEARNED": weights, "CG_B200_PRECISION": "fp64"})
+    assert p.returncode == 1 and "runs in mixed precision" in p.stderr
+    for env in ({"CG_B200_FUSED": "0"}, {"CG_PRECONDITIONER": "none"}):
+        p = run([mtx], dict(env, CG_B200_LEARNED=weights))
+        assert p.returncode == 1 and "needs Jacobi and the fused solve" in p.stderr
