@@ -1096,6 +1096,21 @@ cgx_status cgx_upload_ell(cgx_handle *h, int N, int nz, int maxNz,
   if (N <= 0 || nz < 0 || maxNz < 0 || !length ||
       ((size_t)maxNz * N > 0 && (!index || !data)))
     return fail(CGX_ERROR_INVALID_ARGUMENT, "bad ELL sizes or pointers");
+  // nz sizes the row-layout copies of the mixed and learned paths, so it must
+  // be the number of entries the lengths describe (a well-formed ELL matrix
+  // has it by construction).
+  {
+    long long sum = 0;
+    for (int i = 0; i < N; i++)
+      if (length[i] < 0 || length[i] > maxNz)
+        return fail(CGX_ERROR_INVALID_ARGUMENT,
+                    "invalid ELL matrix: row pointers/lengths out of order or range;");
+      else
+        sum += length[i];
+    if (sum != nz)
+      return fail(CGX_ERROR_INVALID_ARGUMENT,
+                  "invalid ELL matrix: nz differs from the sum of the row lengths");
+  }
   DeviceGuard guard(h->device);
   CUDA_TRY(cudaStreamSynchronize(h->stream));
   free_matrix(h);

@@ -139,7 +139,8 @@ cgx_status cgx_synchronize(cgx_handle *h);
 cgx_status cgx_upload_crs(cgx_handle *h, int N, int nz, const int *ptr,
                           const int *index, const double *value);
 /* ELL as in MatrixDataELL (Matrix.h:74-87): column-major, element (i, j) at
- * j*N + i, length[i] entries used per row, maxNz slots per row. The paths
+ * j*N + i, length[i] entries used per row (0 <= length[i] <= maxNz, summing
+ * to nz), maxNz slots per row. The paths
  * that read rows (mixed, learned, cgx_jacobi_from_matrix) build a CRS copy
  * of it on the device on first use. */
 cgx_status cgx_upload_ell(cgx_handle *h, int N, int nz, int maxNz,

@@ -157,3 +157,23 @@ def test_invalid_matrix_rejected(handle):
     assert e.value.status == 1
     with pytest.raises(cgxx_b200.CgxError):
         handle.upload_crs(np.array([0, 2, 1], np.int32), np.array([0, 1], np.int32), np.ones(2))
+
+
+def test_ell_upload_checks_lengths_against_nz(handle):
+    """nz sizes the row-layout copies that the mixed and learned paths build
+    from an ELL matrix, so an upload whose nz is not the sum of the row
+    lengths, or with a length outside [0, maxNz], is rejected on the host and
+    leaves the previous matrix in place."""
+    import cgxx_b200 as cg
+    from cgxx_b200 import generators as G
+    A = random_crs(257, 0, 9, seed=41)
+    max_nz, length, index, data = G.to_ell(A)
+    handle.upload_ell(A.N, A.nz, max_nz, length, index, data)
+    x = _x(A.N)
+    handle.set_vector("X", x)
+    for nz, lens in ((A.nz + 1, length), (A.nz, np.where(np.arange(A.N) == 5, max_nz + 1, length))):
+        with pytest.raises(cg.CgxError) as e:
+            handle.upload_ell(A.N, nz, max_nz, lens.astype(np.int32), index, data)
+        assert e.value.status == 1 and "invalid ELL matrix" in e.value.message
+    handle.matvec("X", "Q")
+    assert np.array_equal(handle.get_vector("Q"), O.matvec_ell(A.N, length, index, data, x))
