@@ -133,7 +133,7 @@ def workload_config(args, A):
     return {
         "workload": workload_name(args),
         "N": A.N, "nnz": A.nz, "format": "CRS", "preconditioner": "jacobi",
-        "path": args.path, "field": field,
+        "field": field,
         "rhs": "A x*, x* ~ U[-1,1] seed 7", "tolerance": args.tol,
         "max_iterations": args.max_iter, "l2": "inputs larger than L2 (no flush)",
         "parallelism": "replicas" if args.gpus > 1 else "single GPU",
@@ -202,23 +202,30 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # Reference CPU implementation (oracle/_ref, built from the reference sources)
 
-def mtx_cache_path(A, name):
+def mtx_cache_path(A, name, native=False):
+    """The workload as a symmetric MatrixMarket file (cached per machine).
+    native=True writes it with libcgb200's parallel writer (our arm, which
+    loads that library anyway); the reference arm uses the pure-Python
+    writer and maps none of this project's native libraries."""
     os.makedirs(CACHE, exist_ok=True)
     path = os.path.join(CACHE, name.replace("^", "_") + ".mtx")
     if not os.path.exists(path):
         tmp = path + f".tmp{os.getpid()}"
         from cgxx_b200 import generators as G
-        G.write_mtx_symmetric(tmp, A)
+        if native:
+            G.write_mtx_symmetric(tmp, A)
+        else:
+            G.write_mtx_symmetric_py(tmp, A)
         os.replace(tmp, path)
     return path
 
 
-def run_reference(A, b, name, reps, max_iter, tol, threads, backend="omp"):
+def run_reference(A, b, name, reps, max_iter, tol, threads, backend="omp", native=False):
     """Runs the reference's OpenMP (or serial) CG in-process harness on the
     workload with right-hand side b. Returns the list of per-repetition solve
     times (s) and the iteration counts."""
     from oracle import oracle as O
-    path = mtx_cache_path(A, name)
+    path = mtx_cache_path(A, name, native)
     env = {"CG_MAX_ITER": str(max_iter), "CG_TOLERANCE": repr(tol),
            "CG_MATRIX_FORMAT": "CRS", "CG_PRECONDITIONER": "jacobi"}
     if backend == "omp":
@@ -269,7 +276,8 @@ def reference_arm(args, world, rank):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": dict(workload_config(args, A), path="reference OpenMP Jacobi-CG (CRS)"),
+        "config": workload_config(args, A),
+        "path": "reference OpenMP Jacobi-CG (CRS)",
         "iterations": iters[-1],
         "cpu_baseline": {"value": ms, "unit": "ms", "cores": threads, "kind": "reference",
                          "sample": sample},
@@ -571,7 +579,8 @@ def our_arm(args, world, rank, local):
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
             "dtype": {"plain": "f64", "mixed": "f32+f64"}.get(args.path, "bf16+f32+f64"),
             "data": "synthetic (seeded generator; no dataset)",
-            "config": dict(workload_config(args, A), network=net_info),
+            "config": workload_config(args, A),
+            "path": args.path, "network": net_info,
             "iterations": iters, "outer_iterations": outer,
             "residual": res["residual"], "true_residual": true_rel,
             "rel_error_vs_exact": err_vs_exact, "converged": bool(res["converged"]),
@@ -602,7 +611,8 @@ def cpu_baseline(A, b, args, full_iters):
     threads = host_threads()
     sample = 100
     try:
-        times, iters, _ = run_reference(A, b, workload_name(args), 2, sample, args.tol, threads)
+        times, iters, _ = run_reference(A, b, workload_name(args), 2, sample, args.tol, threads,
+                                        native=True)
     except Exception as e:  # pragma: no cover - reported, not fatal
         return {"value": None, "error": str(e)[:200]}
     t = min(times)
@@ -612,18 +622,19 @@ def cpu_baseline(A, b, args, full_iters):
            "sample": f"{iters[-1]} iterations (CG_MAX_ITER={sample}) of the same solve by the "
                      f"reference's CGOpenMP, best of 2, scaled to {full} iterations",
            "ms_per_iteration": per_iter_ms}
-    # The reference's serial CG beside it, on one core: a smaller sample.
+    # The reference's serial CG beside it, on one core: a smaller sample
+    # (an estimate: per-iteration time of the first 50 iterations, scaled).
     if O.ref_binary("ref_harness_serial") is not None:
-        ssample = 10
+        ssample = 50
         try:
             st, si, _ = run_reference(A, b, workload_name(args), 1, ssample, args.tol, 1,
-                                      backend="serial")
+                                      backend="serial", native=True)
             s_ms = 1e3 * min(st) / si[-1]
             out["serial"] = {"value": s_ms * full, "unit": "ms", "cores": 1,
                              "kind": "reference",
                              "sample": f"{si[-1]} iterations (CG_MAX_ITER={ssample}) of the same "
                                        f"solve by the reference's serial CG, scaled to {full} "
-                                       "iterations",
+                                       "iterations (an estimate, not a full solve)",
                              "ms_per_iteration": s_ms}
         except Exception as e:  # pragma: no cover - reported, not fatal
             out["serial"] = {"value": None, "error": str(e)[:200]}

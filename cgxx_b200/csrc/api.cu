@@ -152,6 +152,14 @@ static void band_free(cgx_handle *h, Band &B) {
   B = Band{};
 }
 
+// Releases U after a refresh whose values failed the symmetry check, keeping
+// the planned offsets: a later refresh with symmetric values fills U again.
+static void band_drop_values(cgx_handle *h, Band &B) {
+  if (B.U) dev_free(h, B.U);
+  B.U = nullptr;
+  B.ok = false;
+}
+
 struct cgx_handle {
   int device = 0;
   // Device blocks of replaced matrices, kept for the next upload
@@ -252,7 +260,6 @@ struct Learned {
   float *pre[4] = {};
   float *o = nullptr;
   float *y32 = nullptr, *z32 = nullptr;
-  double *xbak = nullptr;
   // training
   float *V = nullptr, *T1 = nullptr, *T2 = nullptr, *rho = nullptr;
   float *dT2 = nullptr, *dT1 = nullptr, *dg = nullptr, *dO = nullptr;
@@ -1610,7 +1617,7 @@ static cgx_status ensure_f32(cgx_handle *h) {
   }
   if (h->band.K > 0) {
     CGX_TRY(band_fill(h, h->band));
-    if (!h->band.ok) band_free(h, h->band);
+    if (!h->band.ok) band_drop_values(h, h->band);
   }
   if (!h->band.ok && !h->sa_tried) {
     h->sa_tried = true;
@@ -1726,9 +1733,13 @@ static cudaError_t launch_learned_iteration(cgx_handle *h,
 }
 
 // FP32-inner / FP64-refinement solve. The inner preconditioner is Jacobi or
-// the learned factor; with the learned one, an outer step whose FP64 true
-// residual is NaN/Inf or shrinks by less than half is undone (x restored) and
-// the remaining steps use Jacobi (result.fell_back = 1).
+// the learned factor. An outer step whose FP64 true residual is NaN/Inf or
+// shrinks by less than half (the FP32 inner solve broke down or stalled:
+// values beyond the FP32 range, a matrix too ill-conditioned for FP32, a
+// corrupt factor) is undone, x is restored to where the step started, and
+// the solve finishes with plain FP64 Jacobi-CG from there
+// (result.fell_back = 1), the reference's algorithm, with its own budget of
+// max_iterations.
 static cgx_status solve_mixed(cgx_handle *h, const cgx_options &o,
                               cgx_result &res) {
   CGX_TRY(ensure_rows(h));
@@ -1802,8 +1813,11 @@ static cgx_status solve_mixed(cgx_handle *h, const cgx_options &o,
   h->host_st->inner_tol_min = o.inner_tolerance;
   CGX_TRY(push_state(h));
 
-  bool learned = want_learned;
+  const bool learned = want_learned;
+  double *x = h->vec[CGX_VECTOR_X];
+  double *xbak = h->tmp;  // x at the start of the current outer step
   double rel = 0, prev = -1;
+  bool failed = false;
   int outer = 0;
   double t_spmv = 0, t_upd = 0, t_dir = 0;
   int launches = 0;
@@ -1811,24 +1825,22 @@ static cgx_status solve_mixed(cgx_handle *h, const cgx_options &o,
     double r2;
     CGX_TRY(true_residual_r2(h, &r2));
     rel = bnorm > 0 ? std::sqrt(r2) / bnorm : std::sqrt(r2);
-    if (learned && outer > 0 && (!std::isfinite(rel) || rel > 0.5 * prev)) {
-      // The learned step failed: undo it and continue with Jacobi.
-      CUDA_TRY(cudaMemcpyAsync(h->vec[CGX_VECTOR_X], h->L->xbak,
-                               sizeof(double) * h->N, cudaMemcpyDeviceToDevice, s));
-      learned = false;
-      res.fell_back = 1;
-      CGX_TRY(true_residual_r2(h, &r2));
-      rel = bnorm > 0 ? std::sqrt(r2) / bnorm : std::sqrt(r2);
+    if (outer > 0 && (!std::isfinite(rel) || rel > 0.5 * prev)) {
+      // The step failed: undo it; plain FP64 finishes below.
+      CUDA_TRY(cudaMemcpyAsync(x, xbak, sizeof(double) * h->N,
+                               cudaMemcpyDeviceToDevice, s));
+      failed = true;
+      rel = prev;
+      break;
     }
-    if (!(rel > o.tolerance)) break;  // converged (or NaN: stop)
+    if (!(rel > o.tolerance)) break;  // converged (or NaN before any step: stop)
     if (outer >= o.max_outer) break;
     CGX_TRY(pull_state(h));
     if (h->host_st->total_inner >= o.max_iterations) break;
     outer++;
     prev = rel;
-    if (learned)
-      CUDA_TRY(cudaMemcpyAsync(h->L->xbak, h->vec[CGX_VECTOR_X],
-                               sizeof(double) * h->N, cudaMemcpyDeviceToDevice, s));
+    CUDA_TRY(cudaMemcpyAsync(xbak, x, sizeof(double) * h->N,
+                             cudaMemcpyDeviceToDevice, s));
     const double tin = std::max(o.inner_tolerance, 0.5 * o.tolerance / rel);
     // Inner tolerance, graph condition and a fresh loop-guard count.
     h->host_st->in_tol = tin;
@@ -1894,6 +1906,25 @@ static cgx_status solve_mixed(cgx_handle *h, const cgx_options &o,
   CUDA_TRY(cudaEventElapsedTime(&ms, h->ev[6], h->ev[7]));
   res.solve_ms = ms;
   res.iterations = h->host_st->total_inner;
+  if (failed) {
+    // Plain FP64 Jacobi-CG from the restored x. Its tolerance is relative to
+    // the residual it starts from (rel = ||b - A x|| / ||b|| there), with a
+    // factor 2 of margin for the drift between its recurrence residual and
+    // the true one; the FP64 true residual is taken again afterwards.
+    cgx_options fo = o;
+    fo.precision = CGX_PRECISION_FP64;
+    fo.preconditioner = CGX_PRECONDITIONER_JACOBI;
+    fo.tolerance = 0.5 * o.tolerance / rel;
+    cgx_result fr;
+    std::memset(&fr, 0, sizeof(fr));
+    CGX_TRY(solve_fp64(h, fo, fr));
+    double r2;
+    CGX_TRY(true_residual_r2(h, &r2));
+    rel = bnorm > 0 ? std::sqrt(r2) / bnorm : std::sqrt(r2);
+    res.fell_back = 1;
+    res.iterations += fr.iterations;
+    res.solve_ms += fr.solve_ms;
+  }
   res.outer_iterations = outer;
   res.residual = rel;
   res.true_residual = rel;
@@ -1946,7 +1977,6 @@ cgx_status learned_alloc(cgx_handle *h, int nnzL) {
   for (int k = 0; k < 4; k++) o_h[k] = take_n<__nv_bfloat16>(c, (size_t)N * W);
   size_t o_o = take_n<float>(c, (size_t)N * NOUT);
   size_t o_y = take_n<float>(c, N), o_z = take_n<float>(c, N);
-  size_t o_xb = take_n<double>(c, N);
   CUDA_TRY(dev_alloc(h, (void **)&L->mem, c.off));
   CUDA_TRY(cudaMemsetAsync(L->mem, 0, c.off, h->stream));
   char *b = (char *)L->mem;
@@ -1972,7 +2002,6 @@ cgx_status learned_alloc(cgx_handle *h, int nnzL) {
   L->o = (float *)(b + o_o);
   L->y32 = (float *)(b + o_y);
   L->z32 = (float *)(b + o_z);
-  L->xbak = (double *)(b + o_xb);
   return CGX_SUCCESS;
 }
 

@@ -817,6 +817,16 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
+// The inner FP32 iteration cannot make progress: a step length that is zero
+// (<p,q> overflowed to infinity, as with values beyond the FP32 range) or not
+// finite. The stop that follows hands the failed refinement step to the
+// host, which restores x and finishes in FP64. A NaN residual stops the loop
+// through the residual test itself (!(res > tol)).
+__device__ __forceinline__ bool inner_broke_down(const CgState *st) {
+  const double a = st->in_alpha;
+  return !(fabs(a) <= 1.7976931348623157e308) || a == 0.0;
+}
+
 // Inner step 2: r -= a q; partial <r,r>, <r,Cr>; finalize residual test and b.
 __global__ void __launch_bounds__(kThreads)
     k_inner_update(int N, float *__restrict__ r, const float *__restrict__ q,
@@ -861,7 +871,8 @@ __global__ void __launch_bounds__(kThreads)
     st->total_inner += 1;
     const double res = sqrt(out[0]) / st->in_nrm0;
     st->in_res = res;
-    if (res <= st->in_tol || st->total_inner >= st->max_iter) {
+    if (!(res > st->in_tol) || inner_broke_down(st) ||
+        st->total_inner >= st->max_iter) {
       st->in_stop = 1;
     } else {
       const double rho = out[1];
@@ -1032,7 +1043,8 @@ __global__ void __launch_bounds__(kThreads)
     st->total_inner += 1;
     const double res = sqrt(out[0]) / st->in_nrm0;
     st->in_res = res;
-    if (!(res > st->in_tol) || st->total_inner >= st->max_iter)
+    if (!(res > st->in_tol) || inner_broke_down(st) ||
+        st->total_inner >= st->max_iter)
       st->in_stop = 1;
     if (st->use_cond)
       cudaGraphSetConditional((cudaGraphConditionalHandle)st->cond,

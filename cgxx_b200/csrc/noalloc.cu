@@ -74,7 +74,9 @@ __global__ void __launch_bounds__(cgx::kThreads)
 
 // Device address of g_scratch per device, looked up once per device with
 // that device current. In host code the name g_scratch is only a host-side
-// stand-in, never a device address.
+// stand-in, never a device address. The address is kept until the process
+// exits: a cudaDeviceReset may reload the library image elsewhere, and calls
+// on that device after a reset are not supported.
 std::mutex g_mutex;
 constexpr int kMaxDevices = 64;
 NoAllocScratch *g_addr[kMaxDevices] = {};

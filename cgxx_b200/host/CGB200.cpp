@@ -279,12 +279,13 @@ public:
       printPadded("Precision:", precision == CGX_PRECISION_MIXED
                                     ? "FP32 inner / FP64 refinement"
                                     : "FP64");
-      if (precision == CGX_PRECISION_MIXED)
+      if (precision == CGX_PRECISION_MIXED) {
         printPadded("Refinement steps:", std::to_string(last.outer_iterations));
+        printPadded("Fell back to FP64:", last.fell_back ? "yes" : "no");
+      }
       if (gnn) {
         printPadded("Learned factor:", learnedFile);
         printPadded("Learned set-up time:", std::to_string(learnedSetupSeconds));
-        printPadded("Fell back to Jacobi:", last.fell_back ? "yes" : "no");
       }
       static const char *loops[] = {"CUDA graph (while node)",
                                     "CUDA graph chunks", "kernel launches"};

@@ -108,7 +108,15 @@ typedef struct cgx_result {
    * number of launches of each; zero in the other loop modes. */
   double spmv_ms, update_ms, direction_ms;
   int spmv_launches, update_launches, direction_launches;
-  int fell_back;         /* learned preconditioner replaced by Jacobi */
+  int fell_back;         /* MIXED: an FP32 refinement step broke down or
+                            stalled (its FP64 true residual was NaN/Inf or
+                            fell by less than half); it was undone and the
+                            solve finished with plain FP64 Jacobi-CG from the
+                            restored x, with a budget of max_iterations of its
+                            own. iterations then counts both parts. A system
+                            that no budget solves (e.g. singular and
+                            inconsistent) ends with status CGX_SUCCESS and
+                            converged = 0. */
 } cgx_result;
 
 /* Library ------------------------------------------------------------------ */
@@ -313,9 +321,11 @@ void cgx_free(void *p);
  *     (cudaGetSymbolAddress); make that first call before any stream capture.
  *   - All calls share the one array: calls that overlap on the GPU (different
  *     streams, or several host threads) race and give wrong results.
+ *   - The looked-up address is kept for the life of the process. After
+ *     cudaDeviceReset on a device, the library image may load at another
+ *     address, so calls on that device are then invalid.
  * Deterministic: the result depends only on a, b and n.
- * Has no counterpart in the reference (its vectorDotKernel reduces into a
- * cudaMalloc'ed buffer, cuda/CGCUDA.cu:73). */
+ * Has no counterpart in the reference. */
 cgx_status cgx_dot_noalloc(const double *a, const double *b, int n,
                            double *result, void *stream);
 

@@ -290,24 +290,6 @@ def test_learned_solve_on_geometric_graph():
     net.close()
 
 
-def test_corrupted_network_falls_back_to_jacobi():
-    A = G.diffusion3d(16, 7, seed=6)
-    b, _ = G.rhs_for(A, seed=2)
-    h = _setup(A)
-    p = GO.init_params(0)
-    p[GO.param_count() - 1] = np.nan  # poisons the head bias -> NaN factor
-    net = cg.Gnn(0, p)
-    h.learned_factor(net, 0.0)
-    h.set_vector("K", b)
-    r = h.solve(max_iterations=20000, tolerance=1e-9, precision=cg.PRECISION_MIXED,
-                preconditioner=cg.PRECOND_LEARNED)
-    x = h.get_vector("X")
-    assert r["fell_back"] == 1 and r["converged"] == 1
-    assert np.linalg.norm(b - A.matvec(x)) / np.linalg.norm(b) <= 1e-9
-    h.close()
-    net.close()
-
-
 def test_learned_setup_rejects_unsymmetric_pattern():
     N = 50
     rows = np.concatenate([np.arange(N), np.arange(1, N)])

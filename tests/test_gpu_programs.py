@@ -106,5 +106,5 @@ def test_cg_b200_learned_preconditioner(tmp_path):
     s_l, s_j = O.parse_summary(out_l), O.parse_summary(out_j)
     assert s_l["correct"] and s_j["correct"]
     assert s_l["residual"][0] <= 1e-9
-    assert "Fell back to Jacobi:" in out_l and re.search(r"Fell back to Jacobi:\s+no", out_l)
+    assert "Fell back to FP64:" in out_l and re.search(r"Fell back to FP64:\s+no", out_l)
     assert s_l["iterations"][0] < 0.75 * s_j["iterations"][0], (s_l["iterations"], s_j["iterations"])

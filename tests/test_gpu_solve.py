@@ -280,6 +280,31 @@ def test_mixed_on_irregular_patterns(handle, case):
     _check_inner_form(handle, A, _IRREGULAR[case])
 
 
+def test_band_returns_after_an_asymmetric_refresh(handle):
+    """A value refresh that fails the band's symmetry check moves the inner
+    SpMV to SELL-U; a later refresh with symmetric values on the same pattern
+    brings the band back (the planned offsets are kept)."""
+    A = G.diffusion3d(13, stencil=7, seed=14)
+    b, _ = G.rhs_for(A, seed=15)
+    handle.upload_crs(A.ptr, A.index, A.value)
+    forms = []
+    for vals in (A.value, _asymmetric(A).value, A.value * 1.5):
+        handle.update_crs_values(vals)
+        M = G.Crs(A.N, A.ptr, A.index, vals)
+        handle.upload_jacobi(1.0 / M.diagonal())
+        handle.set_vector("K", b)
+        handle.fill_vector("X", 0.0)
+        res = handle.solve(max_iterations=20000, tolerance=1e-9,
+                           precision=cg.PRECISION_MIXED)
+        x = handle.get_vector("X")
+        assert res["converged"] == 1
+        assert np.linalg.norm(b - M.matvec(x)) / np.linalg.norm(b) <= 1e-9
+        forms.append(handle.inner_band())
+    assert forms[0] == _expected_band(A)
+    assert forms[1] == []
+    assert forms[2] == _expected_band(A)
+
+
 def test_time_spmv_measures_the_fused_product(handle):
     """cgx_time_spmv times the solver's own SpMV (FP64 and the FP32 inner
     one) back to back, and a solve afterwards is unaffected."""

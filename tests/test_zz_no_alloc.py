@@ -3,9 +3,9 @@ memory (a framework that owns all device memory, a loop that forbids
 allocation after start-up). It keeps its scratch in a fixed array inside the
 library instead of cudaMalloc'ed memory.
 
-Checked through the C ABI against the existing entry point cgx_dot, on two
-calls in a row (the second call starts from the scratch contents that the
-first left behind). The test buffers are torch tensors owned by the test;
+Checked through the C ABI against the existing entry point cgx_dot and the
+CPU oracle's FP64 dot product, on two calls in a row (the second call starts
+from the scratch contents that the first left behind). The test buffers are torch tensors owned by the test;
 the entry point itself allocates nothing. This file is collected last so
 that a run stopping at the first failure has already run every other test.
 """
@@ -16,16 +16,17 @@ import pytest
 
 import cgxx_b200 as cg
 from cgxx_b200 import _lib
+from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
 
 REL_TOL = 1e-13  # the dot-product tolerance of the other kernel tests
 
 
-def _reference_dot(a, b):
+def _reference_dot(a, b, device=0):
     """cgx_dot (the handle-based entry point) on the same vectors."""
     n = len(a)
-    with cg.Handle(0) as h:
+    with cg.Handle(device) as h:
         ptr = np.arange(n + 1, dtype=np.int32)  # identity pattern, N = n
         h.upload_crs(ptr, np.arange(n, dtype=np.int32), np.ones(n))
         h.set_vector("P", a)
@@ -41,25 +42,43 @@ def _noalloc_dot(a_dev, b_dev, n, out_dev, stream):
                                    C.c_void_p(stream or None)))
 
 
-@pytest.mark.parametrize("n", [1, 4095, 4096, 1_000_003])
-def test_noalloc_dot_matches_cgx_dot_twice(n):
+def _check_twice(n, device):
     import torch
     rng = np.random.default_rng(n)
     a, b = rng.standard_normal(n), rng.standard_normal(n)
-    ref = _reference_dot(a, b)
-    torch.cuda.set_device(0)
-    a_dev = torch.from_numpy(a).cuda()
-    b_dev = torch.from_numpy(b).cuda()
-    out = torch.full((2,), float("nan"), dtype=torch.float64, device="cuda")
-    stream = torch.cuda.current_stream().cuda_stream
+    ref = _reference_dot(a, b, device)
+    oracle = O.dot(a, b)
+    torch.cuda.set_device(device)
+    a_dev = torch.from_numpy(a).cuda(device)
+    b_dev = torch.from_numpy(b).cuda(device)
+    out = torch.full((2,), float("nan"), dtype=torch.float64, device=f"cuda:{device}")
+    stream = torch.cuda.current_stream(device).cuda_stream
     _noalloc_dot(a_dev, b_dev, n, out[0:1], stream)
     _noalloc_dot(a_dev, b_dev, n, out[1:2], stream)
-    torch.cuda.synchronize()
+    torch.cuda.synchronize(device)
     got = out.cpu().numpy()
     scale = max(1.0, float(np.abs(a) @ np.abs(b)))
     for g in got:
         assert abs(g - ref) <= REL_TOL * scale, (g, ref)
+        assert abs(g - oracle) <= REL_TOL * scale, (g, oracle)
     assert got[0] == got[1]  # deterministic across calls
+
+
+@pytest.mark.parametrize("n", [1, 4095, 4096, 1_000_003])
+def test_noalloc_dot_matches_cgx_dot_twice(n):
+    _check_twice(n, 0)
+
+
+def test_noalloc_dot_on_second_device():
+    """The scratch address is looked up per device: a call on device 1 must
+    use device 1's copy of the array."""
+    import torch
+    if torch.cuda.device_count() < 2:
+        pytest.skip("needs a second GPU")
+    try:
+        _check_twice(1_000_003, 1)
+    finally:
+        torch.cuda.set_device(0)
 
 
 def test_noalloc_dot_rejects_oversize_and_bad_arguments():
