@@ -115,6 +115,9 @@ PROTOTYPES = {
     "cgx_host_alloc": [C.POINTER(_P), C.c_size_t],
     "cgx_host_free": [_P],
     "cgx_dot_noalloc": [_P, _P, _I, _P, _P],
+    "cgx_upload_coo_as": [_P, _I, _I, _P, _P, _P, _I],
+    "cgx_download_crs": [_P, _P, _P, _P],
+    "cgx_download_ell": [_P, _PI, _P, _P, _P],
     "cgx_gnn_param_count": [],
     "cgx_gnn_set_probes": [_P, _I, _I, C.c_float, _I],
     "cgx_learned_capture_residual": [_P, _I],
@@ -227,6 +230,46 @@ class Handle:
         V, pV = _arr(V, np.float64)
         check(self._lib.cgx_upload_coo(self._h, N, len(I), pI, pJ, pV))
         self.N = N
+
+    def upload_coo_as(self, N, I, J, V, fmt):
+        """COO entries in file order, converted on the device into `fmt`
+        (FORMAT_COO, FORMAT_CRS or FORMAT_ELL)."""
+        I, pI = _arr(I, np.int32)
+        J, pJ = _arr(J, np.int32)
+        V, pV = _arr(V, np.float64)
+        check(self._lib.cgx_upload_coo_as(self._h, N, len(I), pI, pJ, pV, fmt))
+        self.N = N
+
+    def matrix_info(self):
+        """(N, nz, format) of the uploaded matrix."""
+        N, nz, fmt = C.c_int(0), C.c_int(0), C.c_int(0)
+        check(self._lib.cgx_matrix_info(self._h, C.byref(N), C.byref(nz), C.byref(fmt)))
+        return N.value, nz.value, fmt.value
+
+    def download_crs(self):
+        """The device's row layout (ptr, index, value)."""
+        N, nz, _ = self.matrix_info()
+        ptr = np.empty(N + 1, np.int32)
+        index = np.empty(max(nz, 1), np.int32)
+        value = np.empty(max(nz, 1), np.float64)
+        check(self._lib.cgx_download_crs(self._h, ptr.ctypes.data_as(C.c_void_p),
+                                         index.ctypes.data_as(C.c_void_p),
+                                         value.ctypes.data_as(C.c_void_p)))
+        return ptr, index[:nz], value[:nz]
+
+    def download_ell(self):
+        """The device's ELL matrix in the reference's column-major layout
+        (max_nz, length, index, data); padding slots read 0."""
+        N, _, _ = self.matrix_info()
+        w = C.c_int(0)
+        check(self._lib.cgx_download_ell(self._h, C.byref(w), None, None, None))
+        length = np.empty(N, np.int32)
+        index = np.empty(max(1, w.value * N), np.int32)
+        data = np.empty(max(1, w.value * N), np.float64)
+        check(self._lib.cgx_download_ell(self._h, None, length.ctypes.data_as(C.c_void_p),
+                                         index.ctypes.data_as(C.c_void_p),
+                                         data.ctypes.data_as(C.c_void_p)))
+        return w.value, length, index[:w.value * N], data[:w.value * N]
 
     def upload_jacobi(self, Cdiag):
         Cdiag, pc = _arr(Cdiag, np.float64)

@@ -25,6 +25,7 @@
 
 #include "cgx.h"
 #include "band.cuh"
+#include "ingest.cuh"
 #include "kernels.cuh"
 #include "learned.cuh"
 #include "sell.cuh"
@@ -141,7 +142,8 @@ static void sellu_free(cgx_handle *h, SellU &S) {
 // A fit the layout (planned once per pattern); ok: the values of the last
 // refresh passed the symmetry check and U holds them.
 struct Band {
-  float *U = nullptr;
+  float *U = nullptr;  // slot-major, kBandMaxK slots of ld floats
+  size_t ld = 0;
   int K = 0;
   int d[kBandMaxK] = {};
   bool ok = false;
@@ -201,6 +203,9 @@ struct cgx_handle {
   int16_t *idx16 = nullptr;
   bool compact16 = false;
   float *d32 = nullptr, *r32 = nullptr, *p32 = nullptr, *q32 = nullptr;
+  // Second buffers of the ping-pong pairs (p, r) and z of the fused band
+  // iterations (band.cuh).
+  float *p32b = nullptr, *r32b = nullptr, *z32 = nullptr;
   double *r64 = nullptr;
   bool f32_valid = false;
   // SELL-U copy of A's FP32 values for the inner SpMV (built with the FP32
@@ -253,6 +258,7 @@ struct Learned {
   void *gb_mem = nullptr;
   __nv_bfloat16 *gb_val = nullptr;
   int *g2b = nullptr;
+  size_t gb_ld = 0;
   int gb_d[kBandMaxK] = {};
   bool gb_ok = false;
   __nv_bfloat16 *h[4] = {};
@@ -376,6 +382,7 @@ static void free_matrix(cgx_handle *h) {
   h->tmp = nullptr;
   h->c_valid = false;
   h->value32 = h->C32 = h->d32 = h->r32 = h->p32 = h->q32 = nullptr;
+  h->p32b = h->r32b = h->z32 = nullptr;
   h->r64 = nullptr;
   h->idx16 = nullptr;
   h->compact16 = false;
@@ -626,21 +633,59 @@ static cudaError_t launch_sellu(cgx_handle *h, const SellU &S, const VT *val,
              : launch_sellu_u<VT, 8, false>(h, A, x, op);
 }
 
-template <typename Op>
-static cudaError_t launch_band(cgx_handle *h, const float *x, Op op) {
-  BandView<4> B;
-  B.U = h->band.U;
-  B.N = h->N;
-  for (int k = 0; k < 4; k++) B.d[k] = k < h->band.K ? h->band.d[k] : 0;
-  auto kern = k_band<4, Op>;
+// Persistent kernel over `rows` rows: as many CTAs as fit on the SMs at
+// once, fewer when the 256-row tiles run out.
+template <typename Kern, typename... Args>
+static cudaError_t launch_rows(cgx_handle *h, Kern kern, size_t rows, Args... args) {
   int per_sm = 0;
   cudaError_t e =
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, 0);
   if (e != cudaSuccess) return e;
-  const int grid = std::max(1, std::min(std::min(h->num_sms * std::max(1, per_sm), kMaxGrid),
-                                        (h->N + kThreads - 1) / kThreads));
-  kern<<<grid, kThreads, 0, h->stream>>>(B, x, op, h->st, h->partials);
+  const size_t tiles = (rows + kThreads - 1) / kThreads;
+  const int grid = (int)std::max<size_t>(
+      1, std::min<size_t>(std::min(h->num_sms * std::max(1, per_sm), kMaxGrid), tiles));
+  kern<<<grid, kThreads, 0, h->stream>>>(args...);
   return cudaGetLastError();
+}
+
+static BandView<4> band_view(const cgx_handle *h) {
+  BandView<4> B;
+  B.U = h->band.U;
+  B.ld = h->band.ld;
+  B.N = h->N;
+  for (int k = 0; k < 4; k++) B.d[k] = k < h->band.K ? h->band.d[k] : 0;
+  return B;
+}
+
+// d_1 = 1: the band kernels take the +-1 neighbours from adjacent lanes.
+static bool band_d1(const cgx_handle *h) {
+  return h->band.K >= 2 && h->band.d[1] == 1;
+}
+
+template <typename Op>
+static cudaError_t launch_band(cgx_handle *h, const float *x, Op op) {
+  const BandView<4> B = band_view(h);
+  if (band_d1(h))
+    return launch_rows(h, k_band<true, Op>, h->N, B, x, op, h->st, h->partials);
+  return launch_rows(h, k_band<false, Op>, h->N, B, x, op, h->st, h->partials);
+}
+
+// Step 1 of a fused band inner iteration (band.cuh): p from z and the last
+// p (buffer `parity`, 0 = p32, 1 = p32b) into the other buffer, d's lagged
+// update, q = A p, a.
+static cudaError_t launch_band_dir(cgx_handle *h, int parity, const float *z) {
+  DirArgs a;
+  a.z = z;
+  a.pold = parity ? h->p32b : h->p32;
+  a.pnew = parity ? h->p32 : h->p32b;
+  a.d = h->d32;
+  a.q = h->q32;
+  a.ticket = ticket(h, kTicketInnerQ);
+  a.pnew_slot = parity ? 0 : 1;
+  const BandView<4> B = band_view(h);
+  if (band_d1(h))
+    return launch_rows(h, k_band_dir<true>, h->N, B, a, h->st, h->partials);
+  return launch_rows(h, k_band_dir<false>, h->N, B, a, h->st, h->partials);
 }
 
 static cudaError_t launch_inner_q(cgx_handle *h) {
@@ -659,18 +704,34 @@ static cudaError_t launch_inner_q(cgx_handle *h) {
       h->p32, op);
 }
 
-// Inner FP32 PCG iteration of the mixed path.
-static cudaError_t launch_inner_iteration(cgx_handle *h,
+// Inner FP32 PCG iteration of the mixed path. With A on the band it is the
+// fused two-kernel iteration (band.cuh) on the buffers of `parity`; its
+// kernel-mode segments are (p update + q = A p | r update | nothing).
+static cudaError_t launch_inner_iteration(cgx_handle *h, int parity,
                                           cudaEvent_t *evs = nullptr) {
   cudaError_t e;
+  const int g = grid_stream(h, (size_t)(h->N + 3) / 4);
+  if (h->band.ok) {
+    if (evs) cudaEventRecord(evs[0], h->stream);
+    if ((e = launch_band_dir(h, parity, h->z32)) != cudaSuccess) return e;
+    if (evs) cudaEventRecord(evs[1], h->stream);
+    k_inner_update<true><<<g, kThreads, 0, h->stream>>>(
+        h->N, h->r32, h->q32, h->C32, h->st, h->partials,
+        ticket(h, kTicketInnerUpdate), h->z32);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (evs) {
+      cudaEventRecord(evs[2], h->stream);
+      cudaEventRecord(evs[3], h->stream);
+    }
+    return cudaSuccess;
+  }
   if (evs) cudaEventRecord(evs[0], h->stream);
   e = launch_inner_q(h);
   if (e != cudaSuccess) return e;
   if (evs) cudaEventRecord(evs[1], h->stream);
-  const int g = grid_stream(h, (size_t)(h->N + 3) / 4);
-  k_inner_update<<<g, kThreads, 0, h->stream>>>(
+  k_inner_update<false><<<g, kThreads, 0, h->stream>>>(
       h->N, h->r32, h->q32, h->C32, h->st, h->partials,
-      ticket(h, kTicketInnerUpdate));
+      ticket(h, kTicketInnerUpdate), nullptr);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if (evs) cudaEventRecord(evs[2], h->stream);
   k_inner_direction<<<g, kThreads, 0, h->stream>>>(h->N, h->d32, h->p32,
@@ -1170,39 +1231,228 @@ cgx_status cgx_upload_ell(cgx_handle *h, int N, int nz, int maxNz,
   return check_flag(h, "ELL");
 }
 
-cgx_status cgx_upload_coo(cgx_handle *h, int N, int nz, const int *I,
-                          const int *J, const double *V) {
+static cgx_status need_matrix(cgx_handle *h);
+static cgx_status ensure_rows(cgx_handle *h);
+namespace {
+cudaError_t scan(cgx_handle *h, int n, const int *in, int *out, int *sums);
+}
+
+// COO entries from the host into the row layout on the device (ingest.cuh):
+// validated, stable-sorted by row, so each row keeps its entries in entry
+// order -- the order in which serial/SerialCG.cpp:79-85 adds a row's
+// products and in which DataMatrix<CRS>::convert and DataMatrix<ELL>::convert
+// (Matrix.cpp:203-228, 339-361) lay them out. `format` CRS or COO: the rows
+// become the matrix itself; ELL: the rows are kept as the row layout of the
+// mixed paths and the tile-major ELL of the SpMV is built from them.
+static cgx_status upload_coo_device(cgx_handle *h, int N, int nz, const int *I,
+                                    const int *J, const double *V, int format) {
+  DeviceGuard guard(h->device);
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  free_matrix(h);
+  const char *what = format == CGX_FORMAT_ELL ? "ELL" : format == CGX_FORMAT_CRS ? "CRS" : "COO";
+
+  // The row layout (ptr, index, value), laid out as the CRS upload does.
+  Carver c;
+  const size_t o_ptr = c.take<int>((size_t)N + 1 + kPad);
+  const size_t o_idx = c.take<int>((size_t)nz + kPad);
+  const size_t o_val = c.take<double>((size_t)nz + kPad);
+  void *rows = nullptr;
+  CUDA_TRY(dev_alloc(h, &rows, c.off));
+  int *ptr = (int *)((char *)rows + o_ptr);
+  int *index = (int *)((char *)rows + o_idx);
+  double *value = (double *)((char *)rows + o_val);
+  if (format == CGX_FORMAT_ELL) h->rows_mem = rows;
+  else h->mat_mem = rows;
+  CUDA_TRY(cudaMemsetAsync(rows, 0, c.off, h->stream));
+
+  // Scratch: the entries, two (row, entry) buffers, the per-tile digit
+  // counts and their scan.
+  const int ntiles = std::max(1, (nz + kSortTile - 1) / kSortTile);
+  const int ncount = kRadix * ntiles;
+  const int nsums = (ncount + cgx::learned::kScanBlock - 1) / cgx::learned::kScanBlock;
+  Carver t;
+  const size_t t_i = t.take<int>((size_t)nz + kPad), t_j = t.take<int>((size_t)nz + kPad);
+  const size_t t_v = t.take<double>((size_t)nz + kPad);
+  const size_t t_k0 = t.take<int>((size_t)nz + kPad), t_v0 = t.take<int>((size_t)nz + kPad);
+  const size_t t_k1 = t.take<int>((size_t)nz + kPad), t_v1 = t.take<int>((size_t)nz + kPad);
+  const size_t t_h = t.take<int>((size_t)ncount), t_o = t.take<int>((size_t)ncount + 1);
+  const size_t t_s = t.take<int>((size_t)nsums);
+  void *tmp = nullptr;
+  CUDA_TRY(dev_alloc(h, &tmp, t.off));
+  char *tb = (char *)tmp;
+  int *dI = (int *)(tb + t_i), *dJ = (int *)(tb + t_j);
+  double *dV = (double *)(tb + t_v);
+  int *kbuf[2] = {(int *)(tb + t_k0), (int *)(tb + t_k1)};
+  int *vbuf[2] = {(int *)(tb + t_v0), (int *)(tb + t_v1)};
+  int *hist = (int *)(tb + t_h), *offs = (int *)(tb + t_o), *sums = (int *)(tb + t_s);
+
+  cudaError_t e = cudaMemsetAsync(h->flag, 0, sizeof(int), h->stream);
+  if (e == cudaSuccess && nz > 0) {
+    e = cudaMemcpyAsync(dI, I, sizeof(int) * (size_t)nz, cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(dJ, J, sizeof(int) * (size_t)nz, cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(dV, V, sizeof(double) * (size_t)nz, cudaMemcpyHostToDevice,
+                          h->stream);
+    if (e == cudaSuccess) {
+      k_coo_validate<<<grid_stream(h, nz), kThreads, 0, h->stream>>>(N, nz, dI, dJ, h->flag);
+      e = cudaGetLastError();
+    }
+  }
+  int flag = 0;
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(&flag, h->flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e == cudaSuccess && flag) {
+    dev_free(h, tmp);
+    free_matrix(h);
+    std::string m = std::string("invalid ") + what + " matrix:";
+    if (flag & 1) m += " row index outside [0, N);";
+    if (flag & 2) m += " column index outside [0, N);";
+    return fail(CGX_ERROR_INVALID_ARGUMENT, m);
+  }
+  // The sort: as many 8-bit passes as N - 1 has significant bits (one at
+  // least); pass p sorts stably by bits 8p .. 8p + 7 of the row.
+  const int* keys = dI;
+  const int* order = nullptr;
+  if (e == cudaSuccess && nz > 0) {
+    int bits = 0;
+    while (bits < 31 && ((unsigned)(N - 1) >> bits) != 0u) bits++;
+    const int passes = std::max(1, (bits + 7) / 8);
+    for (int pass = 0; pass < passes && e == cudaSuccess; pass++) {
+      const int shift = 8 * pass;
+      k_sort_hist<<<ntiles, kThreads, 0, h->stream>>>(nz, keys, shift, ntiles, hist);
+      e = cudaGetLastError();
+      if (e == cudaSuccess) e = scan(h, ncount, hist, offs, sums);
+      if (e == cudaSuccess) {
+        k_sort_scatter<<<ntiles, kThreads, 0, h->stream>>>(
+            nz, keys, order, shift, ntiles, offs, kbuf[pass & 1], vbuf[pass & 1]);
+        e = cudaGetLastError();
+      }
+      keys = kbuf[pass & 1];
+      order = vbuf[pass & 1];
+    }
+  }
+  if (e == cudaSuccess) {
+    k_rows_ptr<<<grid_stream(h, (size_t)nz + 1), kThreads, 0, h->stream>>>(
+        N, nz, nz > 0 ? keys : dI, ptr);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess && nz > 0) {
+    k_rows_gather<<<grid_stream(h, nz), kThreads, 0, h->stream>>>(nz, order, dJ, dV,
+                                                                  index, value);
+    e = cudaGetLastError();
+  }
+  std::vector<int> hptr((size_t)N + 1);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(hptr.data(), ptr, sizeof(int) * ((size_t)N + 1),
+                        cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  dev_free(h, tmp);
+  CUDA_TRY(e);
+  h->ptr = ptr;
+  h->index = index;
+  h->value = value;
+  set_tile_caps(h, hptr.data(), N);
+
+  if (format == CGX_FORMAT_ELL) {
+    // Width = the longest row (MatrixDataELL's maxNz, Matrix.cpp:339-361).
+    CUDA_TRY(cudaMemsetAsync(h->flag, 0, sizeof(int), h->stream));
+    k_row_len_max<<<grid_stream(h, N), kThreads, 0, h->stream>>>(N, ptr, h->flag);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(h->host_scalar, h->flag, sizeof(int),
+                             cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    const int width = *(int *)h->host_scalar;
+    const size_t elems = ell_elems(N, width);
+    Carver m;
+    const size_t m_len = m.take<int>((size_t)N + kPad);
+    const size_t m_idx = m.take<int>(elems + kPad);
+    const size_t m_dat = m.take<double>(elems + kPad);
+    CUDA_TRY(dev_alloc(h, (void **)&h->mat_mem, m.off));
+    char *base = (char *)h->mat_mem;
+    h->ell_length = (int *)(base + m_len);
+    h->ell_index = (int *)(base + m_idx);
+    h->ell_data = (double *)(base + m_dat);
+    h->ell_width = width;
+    CUDA_TRY(cudaMemsetAsync(h->mat_mem, 0, m.off, h->stream));
+    k_rows_to_ell<<<grid_stream(h, N), kThreads, 0, h->stream>>>(
+        N, width, ptr, index, value, h->ell_length, h->ell_index, h->ell_data);
+    CUDA_TRY(cudaGetLastError());
+  }
+  h->N = N;
+  h->nz = nz;
+  h->format = format;
+  CGX_TRY(alloc_vectors(h, N));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return CGX_SUCCESS;
+}
+
+cgx_status cgx_upload_coo_as(cgx_handle *h, int N, int nz, const int *I,
+                             const int *J, const double *V, int format) {
   if (!h) return fail(CGX_ERROR_INVALID_ARGUMENT, "handle is NULL");
   if (N <= 0 || nz < 0 || (nz > 0 && (!I || !J || !V)))
     return fail(CGX_ERROR_INVALID_ARGUMENT, "bad COO sizes or pointers");
-  // serial/SerialCG.cpp:79-85 computes y = 0, then y[I[e]] += V[e] * x[J[e]]
-  // for e in entry order, so each row's sum runs over its entries in entry
-  // order. A stable counting sort by row on the host groups the entries that
-  // way; the device then holds the row-grouped layout and runs the CRS SpMV,
-  // which sums each row in storage order: the same products, the same order,
-  // no atomics.
-  std::vector<int> start((size_t)N + 1, 0);
-  for (int e = 0; e < nz; e++) {
-    if (I[e] < 0 || I[e] >= N)
-      return fail(CGX_ERROR_INVALID_ARGUMENT,
-                  "invalid COO matrix: row index outside [0, N)");
-    start[(size_t)I[e] + 1]++;
+  if (format != CGX_FORMAT_COO && format != CGX_FORMAT_CRS && format != CGX_FORMAT_ELL)
+    return fail(CGX_ERROR_INVALID_ARGUMENT, "unknown matrix format");
+  return upload_coo_device(h, N, nz, I, J, V, format);
+}
+
+cgx_status cgx_upload_coo(cgx_handle *h, int N, int nz, const int *I,
+                          const int *J, const double *V) {
+  return cgx_upload_coo_as(h, N, nz, I, J, V, CGX_FORMAT_COO);
+}
+
+cgx_status cgx_download_crs(cgx_handle *h, int *ptr, int *index, double *value) {
+  CGX_TRY(need_matrix(h));
+  DeviceGuard guard(h->device);
+  CGX_TRY(ensure_rows(h));
+  if (ptr)
+    CUDA_TRY(cudaMemcpyAsync(ptr, h->ptr, sizeof(int) * ((size_t)h->N + 1),
+                             cudaMemcpyDeviceToHost, h->stream));
+  if (index && h->nz > 0)
+    CUDA_TRY(cudaMemcpyAsync(index, h->index, sizeof(int) * (size_t)h->nz,
+                             cudaMemcpyDeviceToHost, h->stream));
+  if (value && h->nz > 0)
+    CUDA_TRY(cudaMemcpyAsync(value, h->value, sizeof(double) * (size_t)h->nz,
+                             cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return CGX_SUCCESS;
+}
+
+cgx_status cgx_download_ell(cgx_handle *h, int *max_nz, int *length, int *index,
+                            double *data) {
+  CGX_TRY(need_matrix(h));
+  if (h->format != CGX_FORMAT_ELL)
+    return fail(CGX_ERROR_INVALID_STATE, "the uploaded matrix is not ELL");
+  DeviceGuard guard(h->device);
+  const int N = h->N, W = h->ell_width;
+  if (max_nz) *max_nz = W;
+  if (length)
+    CUDA_TRY(cudaMemcpyAsync(length, h->ell_length, sizeof(int) * (size_t)N,
+                             cudaMemcpyDeviceToHost, h->stream));
+  const size_t celems = (size_t)N * (size_t)W;
+  if ((index || data) && celems > 0) {
+    Carver t;
+    const size_t o_i = t.take<int>(celems), o_d = t.take<double>(celems);
+    void *tmp = nullptr;
+    CUDA_TRY(dev_alloc(h, &tmp, t.off));
+    int *ci = (int *)((char *)tmp + o_i);
+    double *cd = (double *)((char *)tmp + o_d);
+    k_ell_columns<<<grid_stream(h, celems), kThreads, 0, h->stream>>>(
+        N, W, h->ell_length, h->ell_index, h->ell_data, ci, cd);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess && index)
+      e = cudaMemcpyAsync(index, ci, sizeof(int) * celems, cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess && data)
+      e = cudaMemcpyAsync(data, cd, sizeof(double) * celems, cudaMemcpyDeviceToHost,
+                          h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    dev_free(h, tmp);
+    CUDA_TRY(e);
   }
-  for (int i = 0; i < N; i++) start[i + 1] += start[i];
-  std::vector<int> Jr((size_t)(nz > 0 ? nz : 1));
-  std::vector<double> Vr((size_t)(nz > 0 ? nz : 1));
-  {
-    std::vector<int> fill(start.begin(), start.end() - 1);
-    for (int e = 0; e < nz; e++) {
-      const int k = fill[I[e]]++;
-      Jr[k] = J[e];
-      Vr[k] = V[e];
-    }
-  }
-  // upload_rows returns after a stream synchronisation, so the host vectors
-  // outlive the copies.
-  return upload_rows(h, N, nz, start.data(), Jr.data(), Vr.data(),
-                     CGX_FORMAT_COO, "COO");
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return CGX_SUCCESS;
 }
 
 // The row layout (ptr, index, value) that the Jacobi set-up, the FP32 copies
@@ -1541,7 +1791,8 @@ static cgx_status band_plan(cgx_handle *h, Band &B) {
 static cgx_status band_fill(cgx_handle *h, Band &B) {
   const int N = h->N;
   B.ok = false;
-  const size_t bytes = sizeof(float) * (size_t)N * kBandMaxK;
+  B.ld = band_ld(N);
+  const size_t bytes = sizeof(float) * B.ld * kBandMaxK;
   if (!B.U) CUDA_TRY(dev_alloc(h, (void **)&B.U, bytes));
   unsigned long long *counts = nullptr;
   CUDA_TRY(dev_alloc(h, (void **)&counts, 2 * sizeof(unsigned long long)));
@@ -1556,12 +1807,12 @@ static cgx_status band_fill(cgx_handle *h, Band &B) {
   if (e == cudaSuccess) e = cudaMemsetAsync(h->flag, 0, sizeof(int), h->stream);
   if (e == cudaSuccess) {
     k_band_fill<<<grid_stream(h, N), kThreads, 0, h->stream>>>(
-        N, h->ptr, h->index, h->value, o, B.U, counts, h->flag);
+        N, h->ptr, h->index, h->value, o, B.ld, B.U, counts, h->flag);
     e = cudaGetLastError();
   }
   if (e == cudaSuccess) {
     k_band_check<<<grid_stream(h, N), kThreads, 0, h->stream>>>(
-        N, h->ptr, h->index, h->value, o, B.U, counts, h->flag);
+        N, h->ptr, h->index, h->value, o, B.ld, B.U, counts, h->flag);
     e = cudaGetLastError();
   }
   if (e == cudaSuccess)
@@ -1587,6 +1838,9 @@ static cgx_status ensure_f32(cgx_handle *h) {
     size_t o_r = c.take<float>((size_t)N + kPad);
     size_t o_p = c.take<float>((size_t)N + kPad);
     size_t o_q = c.take<float>((size_t)N + kPad);
+    size_t o_pb = c.take<float>((size_t)N + kPad);
+    size_t o_rb = c.take<float>((size_t)N + kPad);
+    size_t o_z = c.take<float>((size_t)N + kPad);
     size_t o_r64 = c.take<double>((size_t)N + kPad);
     size_t o_i16 = c.take<int16_t>((size_t)h->nz + kPad);
     CUDA_TRY(dev_alloc(h, (void **)&h->f32_mem, c.off));
@@ -1598,6 +1852,9 @@ static cgx_status ensure_f32(cgx_handle *h) {
     h->r32 = (float *)(base + o_r);
     h->p32 = (float *)(base + o_p);
     h->q32 = (float *)(base + o_q);
+    h->p32b = (float *)(base + o_pb);
+    h->r32b = (float *)(base + o_rb);
+    h->z32 = (float *)(base + o_z);
     h->r64 = (double *)(base + o_r64);
     h->idx16 = (int16_t *)(base + o_i16);
   }
@@ -1663,21 +1920,23 @@ static cgx_status true_residual_r2(cgx_handle *h, double *r2) {
   return CGX_SUCCESS;
 }
 
-template <bool TRANS, typename Op>
-static cudaError_t launch_gband(cgx_handle *h, const float *x, Op op) {
+static GBandView gband_view(const cgx_handle *h) {
   GBandView B;
   B.val = h->L->gb_val;
+  B.ld = h->L->gb_ld;
   B.N = h->N;
   for (int k = 0; k < kBandMaxK; k++) B.d[k] = h->L->gb_d[k];
-  auto kern = k_gband<TRANS, Op>;
-  int per_sm = 0;
-  cudaError_t e =
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, 0);
-  if (e != cudaSuccess) return e;
-  const int grid = std::max(1, std::min(std::min(h->num_sms * std::max(1, per_sm), kMaxGrid),
-                                        (h->N + kThreads - 1) / kThreads));
-  kern<<<grid, kThreads, 0, h->stream>>>(B, x, op, h->st, h->partials);
-  return cudaGetLastError();
+  return B;
+}
+
+static bool gband_d1(const cgx_handle *h) { return h->L->gb_d[1] == 1; }
+
+template <bool TRANS, typename Op>
+static cudaError_t launch_gband(cgx_handle *h, const float *x, Op op) {
+  const GBandView B = gband_view(h);
+  if (gband_d1(h))
+    return launch_rows(h, k_gband<TRANS, true, Op>, h->N, B, x, op, h->st, h->partials);
+  return launch_rows(h, k_gband<TRANS, false, Op>, h->N, B, x, op, h->st, h->partials);
 }
 
 // z = G (G^T r) + eps C r with <r,z> (start: also p = z and rho).
@@ -1712,9 +1971,37 @@ static cudaError_t launch_learned_start(cgx_handle *h) {
   return launch_learned_apply(h, true);
 }
 
-static cudaError_t launch_learned_iteration(cgx_handle *h,
+// Both A and G on the band: the learned inner iteration runs as the fused
+// three-kernel iteration of band.cuh.
+static bool learned_fused(const cgx_handle *h) {
+  return h->band.ok && h->L && h->L->gb_ok;
+}
+
+// One learned inner iteration. Fused (learned_fused) on the buffers of
+// `parity`, with kernel-mode segments (p update + q = A p | r update +
+// y = G^T r | z = G y + eps C r); otherwise five kernels with segments
+// (q = A p | r update and the apply | p update).
+static cudaError_t launch_learned_iteration(cgx_handle *h, int parity,
                                             cudaEvent_t *evs = nullptr) {
   cudaError_t e;
+  if (learned_fused(h)) {
+    Learned *L = h->L;
+    float *rold = parity ? h->r32b : h->r32, *rnew = parity ? h->r32 : h->r32b;
+    if (evs) cudaEventRecord(evs[0], h->stream);
+    if ((e = launch_band_dir(h, parity, L->z32)) != cudaSuccess) return e;
+    if (evs) cudaEventRecord(evs[1], h->stream);
+    const ResArgs ra{rold, h->q32, rnew, L->y32, ticket(h, kTicketInnerUpdate)};
+    const GBandView B = gband_view(h);
+    e = gband_d1(h) ? launch_rows(h, k_gband_res<true>, h->N, B, ra, h->st, h->partials)
+                    : launch_rows(h, k_gband_res<false>, h->N, B, ra, h->st, h->partials);
+    if (e != cudaSuccess) return e;
+    if (evs) cudaEventRecord(evs[2], h->stream);
+    const OpLearnedZ zop{rnew, h->C32, L->z32, h->p32, L->eps, 0,
+                         ticket(h, kTicketInnerStart)};
+    if ((e = launch_gband<false>(h, L->y32, zop)) != cudaSuccess) return e;
+    if (evs) cudaEventRecord(evs[3], h->stream);
+    return cudaSuccess;
+  }
   if (evs) cudaEventRecord(evs[0], h->stream);
   e = launch_inner_q(h);
   if (e != cudaSuccess) return e;
@@ -1756,41 +2043,53 @@ static cgx_status solve_mixed(cgx_handle *h, const cgx_options &o,
   CUDA_TRY(cudaEventRecord(h->ev[6], s));
   CGX_TRY(ensure_f32(h));
 
-  auto outer_update = [&] {
-    k_outer_update<<<grid_stream(h, h->N), kThreads, 0, h->stream>>>(
-        h->N, h->vec[CGX_VECTOR_X], h->d32, h->st);
+  // Fused band iterations (band.cuh) leave d's last update pending and
+  // alternate their ping-pong buffers, so a graph body runs two of them.
+  const bool fused_j = h->band.ok;
+  const bool fused_l = want_learned && learned_fused(h);
+  auto outer_update = [&](bool pending) {
+    if (pending)
+      k_outer_update_pending<<<grid_stream(h, h->N), kThreads, 0, h->stream>>>(
+          h->N, h->vec[CGX_VECTOR_X], h->d32, h->p32, h->p32b, h->st);
+    else
+      k_outer_update<<<grid_stream(h, h->N), kThreads, 0, h->stream>>>(
+          h->N, h->vec[CGX_VECTOR_X], h->d32, h->st);
     return cudaGetLastError();
   };
   auto guard = [&] {
     k_loop_guard<<<1, 1, 0, h->stream>>>(h->st);
     return cudaGetLastError();
   };
+  auto jacobi_start = [&] {
+    k_inner_start<<<grid_stream(h, h->N), kThreads, 0, h->stream>>>(
+        h->N, h->r64, h->r32, h->d32, h->p32, h->C32, h->st, h->partials,
+        ticket(h, kTicketInnerStart), fused_j ? h->z32 : nullptr);
+    return cudaGetLastError();
+  };
   GraphEntry *gj = nullptr, *gl = nullptr;
   if (o.loop == CGX_LOOP_GRAPH) {
     CGX_TRY(build_while_graph(
-        h, 300,
+        h, fused_j ? 301 : 300, jacobi_start,
         [&] {
-          k_inner_start<<<grid_stream(h, h->N), kThreads, 0, h->stream>>>(
-              h->N, h->r64, h->r32, h->d32, h->p32, h->C32, h->st,
-              h->partials, ticket(h, kTicketInnerStart));
-          return cudaGetLastError();
-        },
-        [&] {
-          cudaError_t e = launch_inner_iteration(h);
+          cudaError_t e = launch_inner_iteration(h, 0);
+          if (e == cudaSuccess && fused_j) e = launch_inner_iteration(h, 1);
           return e != cudaSuccess ? e : guard();
         },
-        outer_update, &gj));
+        [&] { return outer_update(fused_j); }, &gj));
     if (want_learned)
       CGX_TRY(build_while_graph(
-          h, 500, [&] { return launch_learned_start(h); },
+          h, fused_l ? 501 : 500, [&] { return launch_learned_start(h); },
           [&] {
-            cudaError_t e = launch_learned_iteration(h);
+            cudaError_t e = launch_learned_iteration(h, 0);
+            if (e == cudaSuccess && fused_l) e = launch_learned_iteration(h, 1);
             return e != cudaSuccess ? e : guard();
           },
-          outer_update, &gl));
+          [&] { return outer_update(fused_l); }, &gl));
   } else if (o.loop == CGX_LOOP_CHUNKED) {
-    CGX_TRY(build_chunk_graph(h, 400, [&] { return launch_inner_iteration(h); },
-                              &gj));
+    int parity = 0;  // kChunk is even: every chunk starts at parity 0
+    CGX_TRY(build_chunk_graph(
+        h, fused_j ? 401 : 400,
+        [&] { return launch_inner_iteration(h, fused_j ? (parity++ & 1) : 0); }, &gj));
   }
   const unsigned long long cond_j = gj && o.loop == CGX_LOOP_GRAPH ? gj->cond : 0;
   const unsigned long long cond_l = gl ? gl->cond : 0;
@@ -1858,10 +2157,7 @@ static cgx_status solve_mixed(cgx_handle *h, const cgx_options &o,
       if (learned) {
         CUDA_TRY(launch_learned_start(h));
       } else {
-        k_inner_start<<<grid_stream(h, h->N), kThreads, 0, s>>>(
-            h->N, h->r64, h->r32, h->d32, h->p32, h->C32, h->st, h->partials,
-            ticket(h, kTicketInnerStart));
-        CUDA_TRY(cudaGetLastError());
+        CUDA_TRY(jacobi_start());
       }
       if (o.loop == CGX_LOOP_KERNELS) {
         // kChunk iterations per host wait; their kernels skip once the
@@ -1872,9 +2168,9 @@ static cgx_status solve_mixed(cgx_handle *h, const cgx_options &o,
         for (int c = 0; c < maxChunks; c++) {
           for (int j = 0; j < kChunk; j++) {
             if (learned)
-              CUDA_TRY(launch_learned_iteration(h, &h->evpool[4 * j]));
+              CUDA_TRY(launch_learned_iteration(h, j & 1, &h->evpool[4 * j]));
             else
-              CUDA_TRY(launch_inner_iteration(h, &h->evpool[4 * j]));
+              CUDA_TRY(launch_inner_iteration(h, j & 1, &h->evpool[4 * j]));
           }
           CGX_TRY(pull_state(h));
           const int now = h->host_st->total_inner;
@@ -1887,7 +2183,7 @@ static cgx_status solve_mixed(cgx_handle *h, const cgx_options &o,
         const int maxLaunches = o.max_iterations + 2;
         for (int l = 0; l < maxLaunches; l++) {
           if (learned)
-            CUDA_TRY(launch_learned_iteration(h, nullptr));
+            CUDA_TRY(launch_learned_iteration(h, l & 1, nullptr));
           else
             CUDA_TRY(cudaGraphLaunch(gj->exec, s));
           CUDA_TRY(cudaMemcpyAsync(h->host_scalar, &h->st->in_stop, sizeof(int),
@@ -1896,7 +2192,7 @@ static cgx_status solve_mixed(cgx_handle *h, const cgx_options &o,
           if (*(int *)h->host_scalar) break;
         }
       }
-      CUDA_TRY(outer_update());
+      CUDA_TRY(outer_update(learned ? fused_l : fused_j));
     }
   }
   CUDA_TRY(cudaEventRecord(h->ev[7], s));
@@ -2129,10 +2425,12 @@ cgx_status build_sell(cgx_handle *h) {
   // The band copy when A's offsets fit it.
   Band plan;
   CGX_TRY(band_plan(h, plan));
-  if (plan.K > 0) {
+  // The slot map holds k * ld + i in an int.
+  if (plan.K > 0 && band_ld(h->N) * kBandMaxK <= (size_t)INT_MAX) {
     const int N = h->N;
+    L->gb_ld = band_ld(N);
     Carver c;
-    size_t o_v = take_n<__nv_bfloat16>(c, (size_t)N * kBandMaxK);
+    size_t o_v = take_n<__nv_bfloat16>(c, L->gb_ld * kBandMaxK);
     size_t o_m = take_n<int>(c, (size_t)L->nnzL);
     CUDA_TRY(dev_alloc(h, (void **)&L->gb_mem, c.off));
     L->gb_val = (__nv_bfloat16 *)((char *)L->gb_mem + o_v);
@@ -2146,7 +2444,7 @@ cgx_status build_sell(cgx_handle *h) {
     CUDA_TRY(cudaMemsetAsync(L->gb_mem, 0, c.off, h->stream));
     CUDA_TRY(cudaMemsetAsync(h->flag, 0, sizeof(int), h->stream));
     k_gband_map<<<grid_stream(h, L->nnzL), kThreads, 0, h->stream>>>(
-        L->nnzL, L->grow, L->gcol, o, L->g2b, h->flag);
+        L->nnzL, L->grow, L->gcol, o, L->gb_ld, L->g2b, h->flag);
     CUDA_TRY(cudaGetLastError());
     int flag = 0;
     CUDA_TRY(cudaMemcpyAsync(&flag, h->flag, sizeof(int), cudaMemcpyDeviceToHost,
@@ -2786,6 +3084,9 @@ cgx_status cgx_time_spmv(cgx_handle *h, cgx_precision precision, int reps,
   h->host_st->in_stop = 0;
   h->host_st->in_finished = 0;
   h->host_st->use_cond = 0;
+  // The fused band kernel's lagged updates start from a = b = 0.
+  h->host_st->in_alpha = 0.0;
+  h->host_st->in_beta = 0.0;
   CGX_TRY(push_state(h));
   cudaStream_t s = h->stream;
   cudaGraph_t graph = nullptr;
@@ -2797,7 +3098,7 @@ cgx_status cgx_time_spmv(cgx_handle *h, cgx_precision precision, int reps,
             ? launch_spmv(h, h->vec[CGX_VECTOR_P],
                           OpPcgQ{h->vec[CGX_VECTOR_P], h->vec[CGX_VECTOR_Q],
                                  ticket(h, kTicketQ)})
-            : launch_inner_q(h);
+            : h->band.ok ? launch_band_dir(h, 0, h->z32) : launch_inner_q(h);
   const cudaError_t ec = cudaStreamEndCapture(s, &graph);
   if (e == cudaSuccess) e = ec;
   if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);

@@ -41,7 +41,18 @@ struct CgState {
   double inner_tol_min;  // floor of the inner relative tolerance
   int in_iter, in_stop, in_finished;
   int total_inner;
+  int in_pslot;  // fused band iterations: ping-pong buffer of the last p
 };
+
+// The inner FP32 iteration cannot make progress: a step length that is zero
+// (<p,q> overflowed to infinity, as with values beyond the FP32 range) or not
+// finite. The stop that follows hands the failed refinement step to the
+// host, which restores x and finishes in FP64. A NaN residual stops the loop
+// through the residual test itself (!(res > tol)).
+__device__ __forceinline__ bool inner_broke_down(const CgState *st) {
+  const double a = st->in_alpha;
+  return !(fabs(a) <= 1.7976931348623157e308) || a == 0.0;
+}
 
 // --- reductions ------------------------------------------------------------
 

@@ -597,6 +597,11 @@ struct OpInnerQ {
     q[i] = s;
     a.a0 = fma((double)pr.p, (double)s, a.a0);
   }
+  // Row epilogue of a product that has p_i at hand (x = p).
+  __device__ void row_x(int i, float s, Acc &a, float pi) const {
+    q[i] = s;
+    a.a0 = fma((double)pi, (double)s, a.a0);
+  }
   __device__ void finish(Acc &a, CgState *st, double *partials) const {
     double in[1] = {a.a0}, out[1];
     if (grid_reduce<1>(in, partials, ticket, out) && threadIdx.x == 0)
@@ -787,12 +792,14 @@ __global__ void __launch_bounds__(kThreads)
 // Mixed-precision inner solve: FP32 Jacobi-PCG on A d = r / ||r|| with FP64
 // scalars, inside an FP64 refinement loop driven by the host.
 
-// Start: r32 = r64 / ||r64||, d = 0, p = C r32; <r,p>, <r,r>.
+// Start: r32 = r64 / ||r64||, d = 0, p = C r32 (and z = p when z is given,
+// for the fused band iteration); <r,p>, <r,r>; a = b = 0, so that a fused
+// first iteration forms p = z and leaves d at 0.
 __global__ void __launch_bounds__(kThreads)
     k_inner_start(int N, const double *__restrict__ r64, float *__restrict__ r,
                   float *__restrict__ d, float *__restrict__ p,
                   const float *__restrict__ C, CgState *st, double *partials,
-                  unsigned *ticket) {
+                  unsigned *ticket, float *__restrict__ z = nullptr) {
   const double inv = 1.0 / sqrt(st->r2);
   double rp = 0.0, rr = 0.0;
   for (int i = blockIdx.x * kThreads + threadIdx.x; i < N;
@@ -802,6 +809,7 @@ __global__ void __launch_bounds__(kThreads)
     r[i] = ri;
     d[i] = 0.0f;
     p[i] = pi;
+    if (z) z[i] = pi;
     rp = fma((double)ri, (double)pi, rp);
     rr = fma((double)ri, (double)ri, rr);
   }
@@ -809,6 +817,8 @@ __global__ void __launch_bounds__(kThreads)
   if (grid_reduce<2>(in, partials, ticket, out) && threadIdx.x == 0) {
     st->in_rho = out[0];
     st->in_nrm0 = sqrt(out[1]);
+    st->in_alpha = 0.0;
+    st->in_beta = 0.0;
     st->in_iter = 0;
     st->in_stop = 0;
     st->in_finished = 0;
@@ -817,21 +827,14 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
-// The inner FP32 iteration cannot make progress: a step length that is zero
-// (<p,q> overflowed to infinity, as with values beyond the FP32 range) or not
-// finite. The stop that follows hands the failed refinement step to the
-// host, which restores x and finishes in FP64. A NaN residual stops the loop
-// through the residual test itself (!(res > tol)).
-__device__ __forceinline__ bool inner_broke_down(const CgState *st) {
-  const double a = st->in_alpha;
-  return !(fabs(a) <= 1.7976931348623157e308) || a == 0.0;
-}
-
 // Inner step 2: r -= a q; partial <r,r>, <r,Cr>; finalize residual test and b.
+// STORE_Z (the fused band iteration, whose first kernel reads z of
+// neighbouring rows): also z = C r, with the rounding k_inner_direction uses.
+template <bool STORE_Z>
 __global__ void __launch_bounds__(kThreads)
     k_inner_update(int N, float *__restrict__ r, const float *__restrict__ q,
                    const float *__restrict__ C, CgState *st, double *partials,
-                   unsigned *ticket) {
+                   unsigned *ticket, float *__restrict__ z) {
   if (st->in_stop) return;
   const float na = (float)(-st->in_alpha);
   double rr = 0.0, rz = 0.0;
@@ -849,21 +852,25 @@ __global__ void __launch_bounds__(kThreads)
     rv.z = fmaf(na, qv.z, rv.z);
     rv.w = fmaf(na, qv.w, rv.w);
     r4[i] = rv;
+    const float4 zv = make_float4(cv.x * rv.x, cv.y * rv.y, cv.z * rv.z, cv.w * rv.w);
+    if (STORE_Z) reinterpret_cast<float4 *>(z)[i] = zv;
     rr = fma((double)rv.x, (double)rv.x, rr);
     rr = fma((double)rv.y, (double)rv.y, rr);
     rr = fma((double)rv.z, (double)rv.z, rr);
     rr = fma((double)rv.w, (double)rv.w, rr);
-    rz = fma((double)rv.x, (double)(cv.x * rv.x), rz);
-    rz = fma((double)rv.y, (double)(cv.y * rv.y), rz);
-    rz = fma((double)rv.z, (double)(cv.z * rv.z), rz);
-    rz = fma((double)rv.w, (double)(cv.w * rv.w), rz);
+    rz = fma((double)rv.x, (double)zv.x, rz);
+    rz = fma((double)rv.y, (double)zv.y, rz);
+    rz = fma((double)rv.z, (double)zv.z, rz);
+    rz = fma((double)rv.w, (double)zv.w, rz);
   }
   for (int i = 4 * n4 + blockIdx.x * kThreads + threadIdx.x; i < N;
        i += gridDim.x * kThreads) {
     const float ri = fmaf(na, q[i], r[i]);
     r[i] = ri;
+    const float zi = C[i] * ri;
+    if (STORE_Z) z[i] = zi;
     rr = fma((double)ri, (double)ri, rr);
-    rz = fma((double)ri, (double)(C[i] * ri), rz);
+    rz = fma((double)ri, (double)zi, rz);
   }
   double in[2] = {rr, rz}, out[2];
   if (grid_reduce<2>(in, partials, ticket, out) && threadIdx.x == 0) {
@@ -999,6 +1006,8 @@ struct OpLearnedZ {
     if (grid_reduce<1>(in, partials, ticket, out) && threadIdx.x == 0) {
       if (start) {
         st->in_rho = out[0];
+        st->in_alpha = 0.0;  // a fused first iteration: p = z, d stays 0
+        st->in_beta = 0.0;
       } else {
         st->in_beta = out[0] / st->in_rho;
         st->in_rho = out[0];
@@ -1094,6 +1103,22 @@ __global__ void __launch_bounds__(kThreads)
   for (int i = blockIdx.x * kThreads + threadIdx.x; i < N;
        i += gridDim.x * kThreads)
     x[i] = fma(s, (double)d[i], x[i]);
+}
+
+// The same after a fused band inner solve, whose last update of d is still
+// pending: x += ||r64|| (d + a p), with p the buffer of the pair that the
+// last iteration wrote and d + a p rounded as the unfused update rounds it.
+__global__ void __launch_bounds__(kThreads)
+    k_outer_update_pending(int N, double *__restrict__ x,
+                           const float *__restrict__ d,
+                           const float *__restrict__ p0,
+                           const float *__restrict__ p1, const CgState *st) {
+  const double s = sqrt(st->r2);
+  const float a = (float)st->in_alpha;
+  const float *__restrict__ p = st->in_pslot ? p1 : p0;
+  for (int i = blockIdx.x * kThreads + threadIdx.x; i < N;
+       i += gridDim.x * kThreads)
+    x[i] = fma(s, (double)fmaf(a, p[i], d[i]), x[i]);
 }
 
 }  // namespace cgx

@@ -414,8 +414,12 @@ __global__ void k_head(int N, const __nv_bfloat16 *__restrict__ h,
   }
 }
 
-// Values of Ghat on its pattern from the head outputs; optionally the scaled
-// factor G = D^-1/2 Ghat for the apply, in G order and in G^T order.
+// Values of Ghat on its pattern from the head outputs,
+//   Ghat_ii = softplus(dg_i + DIAG_OFFSET),  Ghat_ij = w_ij (a_i + u_i . v_j),
+// with no constant term: a head near zero (the untrained network) gives
+// Ghat = I, i.e. G G^T = D^-1, Jacobi; every off-diagonal value is learned.
+// Optionally the scaled factor G = D^-1/2 Ghat for the apply, in G order and
+// in G^T order.
 __global__ void k_assemble(int nnzL, const int *__restrict__ grow,
                            const int *__restrict__ gcol,
                            const int *__restrict__ g2a,
@@ -440,7 +444,7 @@ __global__ void k_assemble(int nnzL, const int *__restrict__ grow,
 #pragma unroll
       for (int k = 0; k < RANK; k++)
         uv = fmaf(o[i * NOUT + 2 + k], o[j * NOUT + 2 + RANK + k], uv);
-      v = fabsf(ahat[g2a[e]]) * (1.f + o[i * NOUT + 0] + uv);
+      v = fabsf(ahat[g2a[e]]) * (o[i * NOUT + 0] + uv);
     }
     ghat[e] = v;
     if (gbv) {  // the band copy of G (BF16), which serves G and G^T

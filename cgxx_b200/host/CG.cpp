@@ -145,14 +145,19 @@ void CG::init(const char *matrixFile) {
   nz = matrixCOO->nz;
   const auto startConverting = now();
 
+  const bool onDevice = convertsOnDevice();
   if (matrixFormat == MatrixFormatCRS) {
     std::cout << "Converting matrix to CRS format..." << std::endl;
-    allocateMatrixCRS();
-    matrixCRS->convert(*matrixCOO);
+    if (!onDevice) {
+      allocateMatrixCRS();
+      matrixCRS->convert(*matrixCOO);
+    }
   } else if (matrixFormat == MatrixFormatELL) {
     std::cout << "Converting matrix to ELL format..." << std::endl;
-    allocateMatrixELL();
-    matrixELL->convert(*matrixCOO);
+    if (!onDevice) {
+      allocateMatrixELL();
+      matrixELL->convert(*matrixCOO);
+    }
   }
   if (preconditioner == PreconditionerJacobi) {
     std::cout << "Initializing Jacobi preconditioner..." << std::endl;
@@ -171,7 +176,7 @@ void CG::init(const char *matrixFile) {
   allocateX();
   resetX();
 
-  if (matrixFormat != MatrixFormatCOO) matrixCOO.reset();
+  if (matrixFormat != MatrixFormatCOO && !onDevice) matrixCOO.reset();
 }
 
 void CG::resetX() { std::fill(x, x + N, 0.0); }

@@ -105,6 +105,10 @@ protected:
   // Whole-solve hook: return true after solving (x, iteration and residual
   // set), false to let solve() run the per-kernel algorithm.
   virtual bool fusedSolve() { return false; }
+  // A backend that builds the CRS/ELL layout on its device from the COO
+  // entries it uploads returns true; init() then keeps the COO and skips the
+  // host conversion (the conversion time moves into "Transfer to time").
+  virtual bool convertsOnDevice() { return false; }
   // Lets a fused backend report device-measured per-kernel times (seconds).
   void setKernelTimes(double matvecS, double axpyS, double xpayS, double dotS,
                       double precondS);

@@ -118,23 +118,17 @@ class CGB200 : public CG {
   }
 
   bool needsTransfer() override { return true; }
+  // The COO entries go to the device, which sorts them into CRS or ELL
+  // (cgx_upload_coo_as): the same arrays as the host conversion, bit for bit.
+  bool convertsOnDevice() override { return true; }
 
   void doTransferTo() override {
     if (!uploaded) {
-      switch (matrixFormat) {
-      case MatrixFormatCRS:
-        ok(cgx_upload_crs(h, N, nz, matrixCRS->ptr, matrixCRS->index,
-                          matrixCRS->value));
-        break;
-      case MatrixFormatELL:
-        ok(cgx_upload_ell(h, N, nz, matrixELL->maxNz, matrixELL->length,
-                          matrixELL->index, matrixELL->data));
-        break;
-      case MatrixFormatCOO:
-        ok(cgx_upload_coo(h, N, nz, matrixCOO->I.get(), matrixCOO->J.get(),
-                          matrixCOO->V.get()));
-        break;
-      }
+      static const int formats[] = {CGX_FORMAT_COO, CGX_FORMAT_CRS, CGX_FORMAT_ELL};
+      ok(cgx_upload_coo_as(h, N, nz, matrixCOO->I.get(), matrixCOO->J.get(),
+                           matrixCOO->V.get(), formats[matrixFormat]));
+      // Later repetitions reuse the device copy; the host COO is not needed.
+      if (matrixFormat != MatrixFormatCOO) matrixCOO.reset();
       if (preconditioner == PreconditionerJacobi)
         ok(cgx_upload_jacobi(h, jacobi->C));
       ok(cgx_set_vector(h, CGX_VECTOR_K, k));

@@ -170,9 +170,10 @@ def main(argv=None):
 
 def init_params(seed=0):
     """The network's initial parameters: He-normal weights (layer weights
-    halved), a near-zero head so that the untrained factor is
-    Ghat = I + |tril(Ahat)| (the first-order factor the network corrects),
-    zero biases. Same as the oracle's init_params."""
+    halved), a near-zero head, zero biases. The factor's head carries no
+    hand-set prior, so the untrained factor is Ghat ~ I (G G^T ~ D^-1, the
+    Jacobi preconditioner) and training learns every off-diagonal value.
+    Same as the oracle's init_params."""
     W, NIN, NOUT = 32, 4, 10
     rng = np.random.default_rng(seed)
     parts = [rng.normal(0, np.sqrt(2.0 / NIN), (W, NIN)), np.zeros(W)]

@@ -105,7 +105,11 @@ typedef struct cgx_result {
   int outer_iterations;  /* MIXED: refinement steps; 0 otherwise */
   double solve_ms;       /* device time of the solve (CUDA events) */
   /* CGX_LOOP_KERNELS only: device time per fused kernel class (ms) and the
-   * number of launches of each; zero in the other loop modes. */
+   * number of launches of each; zero in the other loop modes. FP64 and the
+   * unfused inner iterations: (q = A p | r update | p update). The fused
+   * inner iterations of the symmetric band form (see cgx_inner_band):
+   * spmv = p update + q = A p; update = r update (+ y = G^T r, learned);
+   * direction = z = G y + eps C r (learned) or 0 (Jacobi). */
   double spmv_ms, update_ms, direction_ms;
   int spmv_launches, update_launches, direction_launches;
   int fell_back;         /* MIXED: an FP32 refinement step broke down or
@@ -155,10 +159,30 @@ cgx_status cgx_upload_ell(cgx_handle *h, int N, int nz, int maxNz,
                           const int *length, const int *index,
                           const double *data);
 /* COO as in MatrixCOO (Matrix.h:22-31), entries in file order. The device
- * holds it grouped by row, each row's entries in file order (the order in
- * which serial/SerialCG.cpp:79-85 adds them), in the CRS layout. */
+ * groups it by row (cgx_upload_coo_as), each row's entries in file order
+ * (the order in which serial/SerialCG.cpp:79-85 adds them), in the CRS
+ * layout. */
 cgx_status cgx_upload_coo(cgx_handle *h, int N, int nz, const int *I,
                           const int *J, const double *V);
+/* MatrixCOO (Matrix.h:22-31, entries in file order) converted on the device
+ * into `format` (a cgx_format): the reference's DataMatrix<CRS>::convert
+ * (Matrix.cpp:203-228) and DataMatrix<ELL>::convert (Matrix.cpp:339-361),
+ * which run on its host, and the row grouping of its COO product
+ * (serial/SerialCG.cpp:79-85). A stable radix sort by row on the device
+ * keeps every row's entries in file order, so the CRS and ELL arrays are the
+ * reference's bit for bit. Row or column indices outside [0, N) return
+ * CGX_ERROR_INVALID_ARGUMENT. cgx_upload_coo is this call with
+ * CGX_FORMAT_COO. */
+cgx_status cgx_upload_coo_as(cgx_handle *h, int N, int nz, const int *I,
+                             const int *J, const double *V, int format);
+/* Read-back of the device's matrix (no counterpart in the reference; for
+ * tests and tools): the row layout (ptr: N + 1, index and value: nz; built
+ * on the device from an ELL upload if needed), and, for ELL uploads, the
+ * reference's column-major arrays (index and data: max_nz * N, element
+ * (i, j) at j * N + i, padding slots 0). Each pointer may be NULL. */
+cgx_status cgx_download_crs(cgx_handle *h, int *ptr, int *index, double *value);
+cgx_status cgx_download_ell(cgx_handle *h, int *max_nz, int *length,
+                            int *index, double *data);
 /* Jacobi::C (Preconditioner.h:12-25), N doubles. */
 cgx_status cgx_upload_jacobi(cgx_handle *h, const double *C);
 /* Computes C[i] = 1 / A_ii on the device from the uploaded matrix, with the
@@ -259,10 +283,13 @@ cgx_status cgx_true_residual(cgx_handle *h, double *rel);
 /* Device time of the solver's SpMV alone (no counterpart in the
  * reference): `reps` back-to-back launches of the fused product the solve
  * runs (FP64: q = A p with <p,q> on the uploaded format; MIXED: the FP32
- * inner q = A p with <p,q>) are captured into a CUDA graph and timed with
- * CUDA events on the handle's stream after one untimed launch of the graph;
- * *us_per_launch is the average. Uses the current P (FP64) or inner p (MIXED)
- * and overwrites Q, the inner q and the solver scalars of the last solve. */
+ * inner q = A p with <p,q>, which on the symmetric band form is the fused
+ * first kernel of the inner iteration, p = z + b p_old, d += a p_old,
+ * q = A p, <p,q>) are captured into a CUDA graph and timed with CUDA events
+ * on the handle's stream after one untimed launch of the graph;
+ * *us_per_launch is the average. Uses the current P (FP64) or inner vectors
+ * (MIXED) and overwrites Q, the inner vectors and the solver scalars of the
+ * last solve. */
 cgx_status cgx_time_spmv(cgx_handle *h, cgx_precision precision, int reps,
                          double *us_per_launch);
 

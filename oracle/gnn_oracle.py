@@ -14,7 +14,7 @@ It states, in torch on the CPU, exactly what the device kernels compute:
   head                  o_i = W_h h_i + b_h = [a, dg, u(4), v(4)]     (FP32)
   factor G (lower triangular on the pattern of tril(A)):
       Ghat_ii = softplus(dg_i + 0.5413)
-      Ghat_ij = w_ij (1 + a_i + u_i . v_j)                     (i > j)
+      Ghat_ij = w_ij (a_i + u_i . v_j)                         (i > j)
       G = D^-1/2 Ghat,   M^-1 = G G^T + eps D^-1
   loss (Hutchinson)     L = ||(Ghat^T Ahat Ghat - I) V||_F^2 / (N S)
                         for S probe columns V.
@@ -160,7 +160,7 @@ def forward(g: Graph, flat):
     a, dg = o[:, 0], o[:, 1]
     u, v = o[:, 2:2 + RANK], o[:, 2 + RANK:]
     gdiag = torch.nn.functional.softplus(dg + DIAG_OFFSET)
-    goff = g.lw * (1.0 + a[g.lr] + (u[g.lr] * v[g.lc]).sum(1))
+    goff = g.lw * (a[g.lr] + (u[g.lr] * v[g.lc]).sum(1))
     return gdiag, goff
 
 

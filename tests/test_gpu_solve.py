@@ -414,7 +414,7 @@ def test_mixed_and_learned_accept_every_format():
             rm = h.solve(max_iterations=5000, tolerance=1e-9, precision=cg.PRECISION_MIXED)
             xm = h.get_vector("X")
             h.learned_setup()
-            net = cg.Gnn(0, LRN.init_params(0))
+            net = cg.Gnn(0, LRN.load_weights(LRN.DEFAULT_WEIGHTS)[0])
             h.learned_factor(net, 1e-4)
             net.close()
             h.fill_vector("X", 0.0)

@@ -1,12 +1,13 @@
-"""What the learned factor starts from, on the CPU (oracle only).
+"""The learned factor against its bounds, on the CPU (oracle only).
 
-The untrained network emits the first-order factor Ghat = I + |tril(Ahat)|.
-On the 7-point diffusion family this already has the quality of the
-factorized sparse approximate inverse (FSAI) on the pattern of tril(A), the
-factor that minimises the Kaporin condition number for that pattern, which
-is why training on this family cannot gain much (the shipped weights are
-selected on held-out PCG iterations). Both need about half the iterations of
-Jacobi-PCG.
+The factor's head carries no hand-set prior: the untrained network (a head
+near zero) emits Ghat close to I, so G G^T is close to D^-1 and PCG needs
+nearly Jacobi's iteration count. Training has to learn the off-diagonal
+values. The reference point for what training
+can reach on the pattern of tril(A) is the factorized sparse approximate
+inverse (FSAI) on that pattern, the factor that minimises the Kaporin
+condition number for it; the shipped weights must reach its quality (and so
+about half of Jacobi's iterations) on a field they were not trained on.
 """
 import numpy as np
 import scipy.sparse as sp
@@ -54,26 +55,40 @@ def fsai_lower(A):
     return sp.csr_matrix((vals, (rows, cols)), shape=(N, N))
 
 
-def test_untrained_factor_matches_fsai_quality():
-    A = G.diffusion3d(16, 7, sigma=1.0, corr_len=8.0, seed=1)
-    S = sp.csr_matrix((A.value, A.index, A.ptr), shape=(A.N, A.N))
-    b, _ = G.rhs_for(A, seed=1)
-    d = S.diagonal()
-    it_jacobi = pcg_iterations(S, b, lambda r: r / d)
-
+def _learned_iterations(A, S, b, d, params):
     g = GO.Graph(A.ptr, A.index, A.value)
-    gdiag, goff = GO.factor(g, GO.init_params(0))
+    gdiag, goff = GO.factor(g, params)
     lr, lc = g.lr.numpy(), g.lc.numpy()
     Ghat = sp.csr_matrix((np.concatenate([gdiag, goff]).astype(np.float64),
                           (np.concatenate([np.arange(A.N), lr]),
                            np.concatenate([np.arange(A.N), lc]))), shape=(A.N, A.N))
     Gm = sp.diags(1.0 / np.sqrt(d)) @ Ghat
     GmT = Gm.T.tocsr()
-    it_untrained = pcg_iterations(S, b, lambda r: Gm @ (GmT @ r) + 1e-4 * r / d)
+    return pcg_iterations(S, b, lambda r: Gm @ (GmT @ r) + 1e-4 * r / d)
 
+
+def _problem():
+    A = G.diffusion3d(16, 7, sigma=1.0, corr_len=8.0, seed=1)
+    S = sp.csr_matrix((A.value, A.index, A.ptr), shape=(A.N, A.N))
+    b, _ = G.rhs_for(A, seed=1)
+    return A, S, b, S.diagonal()
+
+
+def test_untrained_factor_is_close_to_jacobi():
+    A, S, b, d = _problem()
+    it_jacobi = pcg_iterations(S, b, lambda r: r / d)
+    it_untrained = _learned_iterations(A, S, b, d, GO.init_params(0))
+    assert 0.8 * it_jacobi <= it_untrained <= it_jacobi + 2, (it_untrained, it_jacobi)
+
+
+def test_shipped_weights_reach_fsai_quality():
+    from cgxx_b200 import learned as LRN
+    A, S, b, d = _problem()
+    params, _ = LRN.load_weights(LRN.DEFAULT_WEIGHTS)
+    it_jacobi = pcg_iterations(S, b, lambda r: r / d)
+    it_trained = _learned_iterations(A, S, b, d, params)
     Gf = fsai_lower(S)
     GfT = Gf.T.tocsr()
     it_fsai = pcg_iterations(S, b, lambda r: Gf @ (GfT @ r))
-
-    assert abs(it_untrained - it_fsai) <= 2, (it_untrained, it_fsai)
-    assert it_untrained <= 0.6 * it_jacobi, (it_untrained, it_jacobi)
+    assert it_trained <= it_fsai + max(2, 0.05 * it_fsai), (it_trained, it_fsai)
+    assert it_trained <= 0.6 * it_jacobi, (it_trained, it_jacobi)
