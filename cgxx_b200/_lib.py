@@ -24,7 +24,7 @@ VECTORS = {"K": 0, "X": 1, "P": 2, "Q": 3, "R": 4, "Z": 5}
 FORMAT_COO, FORMAT_CRS, FORMAT_ELL = range(3)
 PRECOND_NONE, PRECOND_JACOBI, PRECOND_LEARNED = range(3)
 PRECISION_FP64, PRECISION_MIXED = range(2)
-LOOP_GRAPH, LOOP_CHUNKED, LOOP_KERNELS = range(3)
+LOOP_GRAPH, LOOP_CHUNKED, LOOP_KERNELS, LOOP_PERSISTENT = range(4)
 
 
 class Options(C.Structure):

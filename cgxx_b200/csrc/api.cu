@@ -28,7 +28,9 @@
 #include "ingest.cuh"
 #include "kernels.cuh"
 #include "learned.cuh"
+#include "persist.cuh"
 #include "sell.cuh"
+#include "stencil.cuh"
 
 using namespace cgx;
 
@@ -142,8 +144,7 @@ static void sellu_free(cgx_handle *h, SellU &S) {
 // A fit the layout (planned once per pattern); ok: the values of the last
 // refresh passed the symmetry check and U holds them.
 struct Band {
-  float *U = nullptr;  // slot-major, kBandMaxK slots of ld floats
-  size_t ld = 0;
+  float *U = nullptr;  // N x kBandMaxK, row-major
   int K = 0;
   int d[kBandMaxK] = {};
   bool ok = false;
@@ -206,6 +207,9 @@ struct cgx_handle {
   // Second buffers of the ping-pong pairs (p, r) and z of the fused band
   // iterations (band.cuh).
   float *p32b = nullptr, *r32b = nullptr, *z32 = nullptr;
+  // Partial sums and the barrier counter of the persistent inner solves.
+  double *persist_part = nullptr;
+  unsigned long long *persist_sync = nullptr;
   double *r64 = nullptr;
   bool f32_valid = false;
   // SELL-U copy of A's FP32 values for the inner SpMV (built with the FP32
@@ -258,7 +262,6 @@ struct Learned {
   void *gb_mem = nullptr;
   __nv_bfloat16 *gb_val = nullptr;
   int *g2b = nullptr;
-  size_t gb_ld = 0;
   int gb_d[kBandMaxK] = {};
   bool gb_ok = false;
   __nv_bfloat16 *h[4] = {};
@@ -383,6 +386,8 @@ static void free_matrix(cgx_handle *h) {
   h->c_valid = false;
   h->value32 = h->C32 = h->d32 = h->r32 = h->p32 = h->q32 = nullptr;
   h->p32b = h->r32b = h->z32 = nullptr;
+  h->persist_part = nullptr;
+  h->persist_sync = nullptr;
   h->r64 = nullptr;
   h->idx16 = nullptr;
   h->compact16 = false;
@@ -651,41 +656,66 @@ static cudaError_t launch_rows(cgx_handle *h, Kern kern, size_t rows, Args... ar
 static BandView<4> band_view(const cgx_handle *h) {
   BandView<4> B;
   B.U = h->band.U;
-  B.ld = h->band.ld;
   B.N = h->N;
   for (int k = 0; k < 4; k++) B.d[k] = k < h->band.K ? h->band.d[k] : 0;
   return B;
 }
 
-// d_1 = 1: the band kernels take the +-1 neighbours from adjacent lanes.
-static bool band_d1(const cgx_handle *h) {
-  return h->band.K >= 2 && h->band.d[1] == 1;
-}
-
 template <typename Op>
 static cudaError_t launch_band(cgx_handle *h, const float *x, Op op) {
-  const BandView<4> B = band_view(h);
-  if (band_d1(h))
-    return launch_rows(h, k_band<true, Op>, h->N, B, x, op, h->st, h->partials);
-  return launch_rows(h, k_band<false, Op>, h->N, B, x, op, h->st, h->partials);
+  return launch_rows(h, k_band<4, Op>, h->N, band_view(h), x, op, h->st, h->partials);
 }
 
-// Step 1 of a fused band inner iteration (band.cuh): p from z and the last
-// p (buffer `parity`, 0 = p32, 1 = p32b) into the other buffer, d's lagged
-// update, q = A p, a.
-static cudaError_t launch_band_dir(cgx_handle *h, int parity, const float *z) {
-  DirArgs a;
-  a.z = z;
-  a.pold = parity ? h->p32b : h->p32;
-  a.pnew = parity ? h->p32 : h->p32b;
-  a.d = h->d32;
-  a.q = h->q32;
-  a.ticket = ticket(h, kTicketInnerQ);
-  a.pnew_slot = parity ? 0 : 1;
-  const BandView<4> B = band_view(h);
-  if (band_d1(h))
-    return launch_rows(h, k_band_dir<true>, h->N, B, a, h->st, h->partials);
-  return launch_rows(h, k_band_dir<false>, h->N, B, a, h->st, h->partials);
+// The z-marching kernels are switched off until their loads are pipelined:
+// one plane at a time, each step waits a full memory latency (92 us for the
+// fused product at 160^3 against 31 us for the generic kernels).
+constexpr bool kStencilOn = false;
+
+// The z-marching kernels (stencil.cuh) apply when A is on the band and its
+// offsets are those of a 3-D (or 2-D) grid numbered x fastest: 0, 1, nx,
+// nx ny (or 0, 1, nx). The planes are cut into chunks so that the grid holds
+// about six CTAs per SM, and never more CTAs than the partial-sum slots.
+static bool stencil_geom(const cgx_handle *h, StencilGeom *g) {
+  if (!kStencilOn) return false;
+  const Band &B = h->band;
+  if (!B.ok || B.K < 3 || B.d[1] != 1 || B.d[2] < 2) return false;
+  const int nx = B.d[2];
+  long long plane;
+  if (B.K == 3) {
+    plane = h->N;
+  } else {
+    if (B.d[3] % nx != 0) return false;
+    plane = B.d[3];
+  }
+  if (plane % nx != 0 || h->N % plane != 0) return false;
+  g->nx = nx;
+  g->ny = (int)(plane / nx);
+  g->nz = (int)(h->N / plane);
+  g->tiles_x = (g->nx + kStX - 1) / kStX;
+  g->tiles_y = (g->ny + kStY - 1) / kStY;
+  const long long tiles = (long long)g->tiles_x * g->tiles_y;
+  if (tiles > kMaxGrid) return false;
+  const long long want = std::min<long long>(6LL * h->num_sms, kMaxGrid);
+  const int chunks = (int)std::max<long long>(
+      1, std::min<long long>({(long long)g->nz, (want + tiles - 1) / tiles, kMaxGrid / tiles}));
+  g->lz = (g->nz + chunks - 1) / chunks;
+  return true;
+}
+
+static int stencil_grid(const StencilGeom &g) {
+  return st_items(g);
+}
+
+// Step 1 of a fused band inner iteration (stencil.cuh): p from z and the
+// last p (buffer `parity`: 0 = p32, 1 = p32b) into the other buffer, the
+// lagged update of d, q = A p, a.
+static cudaError_t launch_st_dir(cgx_handle *h, const StencilGeom &g, int parity,
+                                 const float *z) {
+  const StDirArgs a{z, parity ? h->p32b : h->p32, parity ? h->p32 : h->p32b, h->d32,
+                    h->q32, ticket(h, kTicketInnerQ), parity ? 0 : 1};
+  k_st_dir<<<stencil_grid(g), kThreads, 0, h->stream>>>(g, band_view(h), a, h->st,
+                                                        h->partials);
+  return cudaGetLastError();
 }
 
 static cudaError_t launch_inner_q(cgx_handle *h) {
@@ -704,16 +734,18 @@ static cudaError_t launch_inner_q(cgx_handle *h) {
       h->p32, op);
 }
 
-// Inner FP32 PCG iteration of the mixed path. With A on the band it is the
-// fused two-kernel iteration (band.cuh) on the buffers of `parity`; its
-// kernel-mode segments are (p update + q = A p | r update | nothing).
+// Inner FP32 PCG iteration of the mixed path. With A on the band of a grid
+// (stencil_geom) it is the fused two-kernel iteration of stencil.cuh on the
+// buffers of `parity`; its kernel-mode segments are (p update + q = A p |
+// r update | nothing).
 static cudaError_t launch_inner_iteration(cgx_handle *h, int parity,
                                           cudaEvent_t *evs = nullptr) {
   cudaError_t e;
   const int g = grid_stream(h, (size_t)(h->N + 3) / 4);
-  if (h->band.ok) {
+  StencilGeom sg;
+  if (stencil_geom(h, &sg)) {
     if (evs) cudaEventRecord(evs[0], h->stream);
-    if ((e = launch_band_dir(h, parity, h->z32)) != cudaSuccess) return e;
+    if ((e = launch_st_dir(h, sg, parity, h->z32)) != cudaSuccess) return e;
     if (evs) cudaEventRecord(evs[1], h->stream);
     k_inner_update<true><<<g, kThreads, 0, h->stream>>>(
         h->N, h->r32, h->q32, h->C32, h->st, h->partials,
@@ -1622,6 +1654,10 @@ static cgx_status device_errors(cgx_handle *h) {
   if (h->host_st->error & 2)
     return fail(CGX_ERROR_DEVICE,
                 "the device loop guard stopped a loop that did not terminate");
+  if (h->host_st->error & kErrGridSync)
+    return fail(CGX_ERROR_DEVICE,
+                "a grid barrier of the persistent inner solve timed out; results are invalid");
+
   return CGX_SUCCESS;
 }
 
@@ -1660,8 +1696,10 @@ static cgx_status solve_fp64(cgx_handle *h, const cgx_options &o,
   if (jacobi && !h->c_valid)
     return fail(CGX_ERROR_INVALID_STATE, "Jacobi preconditioner not set");
   cudaStream_t s = h->stream;
+  // The persistent mode is an inner-solve mode of the mixed paths.
+  const int loop = o.loop == CGX_LOOP_PERSISTENT ? CGX_LOOP_GRAPH : o.loop;
 
-  if (o.loop == CGX_LOOP_GRAPH) {
+  if (loop == CGX_LOOP_GRAPH) {
     GraphEntry *ge = nullptr;
     const int key = 100 + (jacobi ? 1 : 0);
     CGX_TRY(build_while_graph(
@@ -1682,7 +1720,7 @@ static cgx_status solve_fp64(cgx_handle *h, const cgx_options &o,
     float ms = 0;
     CUDA_TRY(cudaEventElapsedTime(&ms, h->ev[0], h->ev[1]));
     res.solve_ms = ms;
-  } else if (o.loop == CGX_LOOP_CHUNKED) {
+  } else if (loop == CGX_LOOP_CHUNKED) {
     GraphEntry *ge = nullptr;
     const int key = 200 + (jacobi ? 1 : 0);
     CGX_TRY(build_chunk_graph(
@@ -1791,8 +1829,7 @@ static cgx_status band_plan(cgx_handle *h, Band &B) {
 static cgx_status band_fill(cgx_handle *h, Band &B) {
   const int N = h->N;
   B.ok = false;
-  B.ld = band_ld(N);
-  const size_t bytes = sizeof(float) * B.ld * kBandMaxK;
+  const size_t bytes = sizeof(float) * (size_t)N * kBandMaxK;
   if (!B.U) CUDA_TRY(dev_alloc(h, (void **)&B.U, bytes));
   unsigned long long *counts = nullptr;
   CUDA_TRY(dev_alloc(h, (void **)&counts, 2 * sizeof(unsigned long long)));
@@ -1807,12 +1844,12 @@ static cgx_status band_fill(cgx_handle *h, Band &B) {
   if (e == cudaSuccess) e = cudaMemsetAsync(h->flag, 0, sizeof(int), h->stream);
   if (e == cudaSuccess) {
     k_band_fill<<<grid_stream(h, N), kThreads, 0, h->stream>>>(
-        N, h->ptr, h->index, h->value, o, B.ld, B.U, counts, h->flag);
+        N, h->ptr, h->index, h->value, o, B.U, counts, h->flag);
     e = cudaGetLastError();
   }
   if (e == cudaSuccess) {
     k_band_check<<<grid_stream(h, N), kThreads, 0, h->stream>>>(
-        N, h->ptr, h->index, h->value, o, B.ld, B.U, counts, h->flag);
+        N, h->ptr, h->index, h->value, o, B.U, counts, h->flag);
     e = cudaGetLastError();
   }
   if (e == cudaSuccess)
@@ -1842,6 +1879,8 @@ static cgx_status ensure_f32(cgx_handle *h) {
     size_t o_rb = c.take<float>((size_t)N + kPad);
     size_t o_z = c.take<float>((size_t)N + kPad);
     size_t o_r64 = c.take<double>((size_t)N + kPad);
+    size_t o_pp = c.take<double>((size_t)kPersistSlots * kMaxGrid);
+    size_t o_ps = c.take<unsigned long long>(1);
     size_t o_i16 = c.take<int16_t>((size_t)h->nz + kPad);
     CUDA_TRY(dev_alloc(h, (void **)&h->f32_mem, c.off));
     CUDA_TRY(cudaMemsetAsync(h->f32_mem, 0, c.off, h->stream));
@@ -1856,6 +1895,8 @@ static cgx_status ensure_f32(cgx_handle *h) {
     h->r32b = (float *)(base + o_rb);
     h->z32 = (float *)(base + o_z);
     h->r64 = (double *)(base + o_r64);
+    h->persist_part = (double *)(base + o_pp);
+    h->persist_sync = (unsigned long long *)(base + o_ps);
     h->idx16 = (int16_t *)(base + o_i16);
   }
   k_to_f32<<<grid_stream(h, h->nz), kThreads, 0, h->stream>>>(
@@ -1923,20 +1964,15 @@ static cgx_status true_residual_r2(cgx_handle *h, double *r2) {
 static GBandView gband_view(const cgx_handle *h) {
   GBandView B;
   B.val = h->L->gb_val;
-  B.ld = h->L->gb_ld;
   B.N = h->N;
   for (int k = 0; k < kBandMaxK; k++) B.d[k] = h->L->gb_d[k];
   return B;
 }
 
-static bool gband_d1(const cgx_handle *h) { return h->L->gb_d[1] == 1; }
-
 template <bool TRANS, typename Op>
 static cudaError_t launch_gband(cgx_handle *h, const float *x, Op op) {
-  const GBandView B = gband_view(h);
-  if (gband_d1(h))
-    return launch_rows(h, k_gband<TRANS, true, Op>, h->N, B, x, op, h->st, h->partials);
-  return launch_rows(h, k_gband<TRANS, false, Op>, h->N, B, x, op, h->st, h->partials);
+  return launch_rows(h, k_gband<TRANS, Op>, h->N, gband_view(h), x, op, h->st,
+                     h->partials);
 }
 
 // z = G (G^T r) + eps C r with <r,z> (start: also p = z and rho).
@@ -1962,6 +1998,49 @@ static cudaError_t launch_learned_apply(cgx_handle *h, bool start) {
   return launch_crs_view(h, Gv, L->y32, zop);
 }
 
+// One inner solve as a persistent cooperative launch (persist.cuh), after
+// the path's start kernel(s). The grid is what the SMs hold at once, as a
+// cooperative launch requires (and no more CTAs than work items or
+// partial-sum slots).
+static cudaError_t launch_inner_persist(cgx_handle *h, const StencilGeom &g, bool learned) {
+  PersistArgs a;
+  a.p[0] = h->p32;
+  a.p[1] = h->p32b;
+  a.r[0] = h->r32;
+  a.r[1] = h->r32b;
+  a.z = learned ? h->L->z32 : h->z32;
+  a.d = h->d32;
+  a.q = h->q32;
+  a.y = learned ? h->L->y32 : nullptr;
+  a.C = h->C32;
+  a.eps = learned ? h->L->eps : 0.f;
+  a.part = h->persist_part;
+  a.sync = h->persist_sync;
+  BandView<4> A = band_view(h);
+  GBandView G{};
+  if (learned) G = gband_view(h);
+  StencilGeom gg = g;
+  void (*kern)(StencilGeom, BandView<4>, GBandView, PersistArgs, CgState *) =
+      learned ? k_inner_persist<true> : k_inner_persist<false>;
+  int per_sm = 0;
+  cudaError_t e =
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, 0);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) return cudaErrorCooperativeLaunchTooLarge;
+  const int grid = std::max(1, std::min({h->num_sms * per_sm, kMaxGrid, st_items(g)}));
+  e = cudaMemsetAsync(a.sync, 0, sizeof(unsigned long long), h->stream);
+  if (e != cudaSuccess) return e;
+  CgState *st = h->st;
+  void *args[] = {&gg, &A, &G, &a, &st};
+  return cudaLaunchCooperativeKernel((const void *)kern, grid, kThreads, args, 0,
+                                     h->stream);
+}
+
+// The default loop mode runs the persistent inner solve where it measured
+// faster than the graph of per-phase kernels: grids whose inner vectors and
+// values stay in L2 (up to 2M rows).
+static bool persist_pays(const cgx_handle *h) { return h->N <= (2 << 20); }
+
 static cudaError_t launch_learned_start(cgx_handle *h) {
   k_inner_start_z<<<grid_stream(h, h->N), kThreads, 0, h->stream>>>(
       h->N, h->r64, h->r32, h->d32, h->st, h->partials,
@@ -1971,10 +2050,13 @@ static cudaError_t launch_learned_start(cgx_handle *h) {
   return launch_learned_apply(h, true);
 }
 
-// Both A and G on the band: the learned inner iteration runs as the fused
-// three-kernel iteration of band.cuh.
-static bool learned_fused(const cgx_handle *h) {
-  return h->band.ok && h->L && h->L->gb_ok;
+// Both A and G on the band of a grid: the learned inner iteration runs as
+// the fused three-kernel iteration of stencil.cuh.
+static bool learned_fused(const cgx_handle *h, StencilGeom *g) {
+  if (!(h->L && h->L->gb_ok) || !stencil_geom(h, g)) return false;
+  for (int k = 0; k < kBandMaxK; k++)
+    if (h->L->gb_d[k] != (k < h->band.K ? h->band.d[k] : 0)) return false;
+  return true;
 }
 
 // One learned inner iteration. Fused (learned_fused) on the buffers of
@@ -1984,21 +2066,23 @@ static bool learned_fused(const cgx_handle *h) {
 static cudaError_t launch_learned_iteration(cgx_handle *h, int parity,
                                             cudaEvent_t *evs = nullptr) {
   cudaError_t e;
-  if (learned_fused(h)) {
+  StencilGeom sg;
+  if (learned_fused(h, &sg)) {
     Learned *L = h->L;
     float *rold = parity ? h->r32b : h->r32, *rnew = parity ? h->r32 : h->r32b;
+    const int grid = stencil_grid(sg);
     if (evs) cudaEventRecord(evs[0], h->stream);
-    if ((e = launch_band_dir(h, parity, L->z32)) != cudaSuccess) return e;
+    if ((e = launch_st_dir(h, sg, parity, L->z32)) != cudaSuccess) return e;
     if (evs) cudaEventRecord(evs[1], h->stream);
-    const ResArgs ra{rold, h->q32, rnew, L->y32, ticket(h, kTicketInnerUpdate)};
-    const GBandView B = gband_view(h);
-    e = gband_d1(h) ? launch_rows(h, k_gband_res<true>, h->N, B, ra, h->st, h->partials)
-                    : launch_rows(h, k_gband_res<false>, h->N, B, ra, h->st, h->partials);
-    if (e != cudaSuccess) return e;
+    const StResArgs ra{rold, h->q32, rnew, L->y32, ticket(h, kTicketInnerUpdate)};
+    k_st_res<<<grid, kThreads, 0, h->stream>>>(sg, gband_view(h), ra, h->st, h->partials);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if (evs) cudaEventRecord(evs[2], h->stream);
     const OpLearnedZ zop{rnew, h->C32, L->z32, h->p32, L->eps, 0,
                          ticket(h, kTicketInnerStart)};
-    if ((e = launch_gband<false>(h, L->y32, zop)) != cudaSuccess) return e;
+    k_st_gz<OpLearnedZ><<<grid, kThreads, 0, h->stream>>>(sg, gband_view(h), L->y32, zop,
+                                                           h->st, h->partials);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if (evs) cudaEventRecord(evs[3], h->stream);
     return cudaSuccess;
   }
@@ -2045,8 +2129,16 @@ static cgx_status solve_mixed(cgx_handle *h, const cgx_options &o,
 
   // Fused band iterations (band.cuh) leave d's last update pending and
   // alternate their ping-pong buffers, so a graph body runs two of them.
-  const bool fused_j = h->band.ok;
-  const bool fused_l = want_learned && learned_fused(h);
+  StencilGeom sg;
+  const bool fused_j = stencil_geom(h, &sg);
+  const bool fused_l = want_learned && learned_fused(h, &sg);
+  // The persistent inner solve (persist.cuh) on a grid's band form.
+  const bool persist = (want_learned ? fused_l : fused_j) &&
+                       (o.loop == CGX_LOOP_PERSISTENT ||
+                        (o.loop == CGX_LOOP_GRAPH && persist_pays(h)));
+  // PERSISTENT on a matrix without a grid band form runs as GRAPH.
+  const bool graph_loop =
+      (o.loop == CGX_LOOP_GRAPH || o.loop == CGX_LOOP_PERSISTENT) && !persist;
   auto outer_update = [&](bool pending) {
     if (pending)
       k_outer_update_pending<<<grid_stream(h, h->N), kThreads, 0, h->stream>>>(
@@ -2067,7 +2159,7 @@ static cgx_status solve_mixed(cgx_handle *h, const cgx_options &o,
     return cudaGetLastError();
   };
   GraphEntry *gj = nullptr, *gl = nullptr;
-  if (o.loop == CGX_LOOP_GRAPH) {
+  if (graph_loop) {
     CGX_TRY(build_while_graph(
         h, fused_j ? 301 : 300, jacobi_start,
         [&] {
@@ -2091,7 +2183,7 @@ static cgx_status solve_mixed(cgx_handle *h, const cgx_options &o,
         h, fused_j ? 401 : 400,
         [&] { return launch_inner_iteration(h, fused_j ? (parity++ & 1) : 0); }, &gj));
   }
-  const unsigned long long cond_j = gj && o.loop == CGX_LOOP_GRAPH ? gj->cond : 0;
+  const unsigned long long cond_j = gj && graph_loop ? gj->cond : 0;
   const unsigned long long cond_l = gl ? gl->cond : 0;
 
   // ||b||.
@@ -2106,8 +2198,7 @@ static cgx_status solve_mixed(cgx_handle *h, const cgx_options &o,
     CUDA_TRY(cudaStreamSynchronize(s));
     bnorm = std::sqrt(h->host_scalar[0]);
   }
-  reset_host_state(h, o.max_iterations, o.tolerance, o.loop == CGX_LOOP_GRAPH,
-                   cond_j);
+  reset_host_state(h, o.max_iterations, o.tolerance, graph_loop, cond_j);
   h->host_st->bnorm = bnorm;
   h->host_st->inner_tol_min = o.inner_tolerance;
   CGX_TRY(push_state(h));
@@ -2151,7 +2242,11 @@ static cgx_status solve_mixed(cgx_handle *h, const cgx_options &o,
                              sizeof(int), cudaMemcpyHostToDevice, s));
     CUDA_TRY(cudaMemcpyAsync(&h->st->cond, &h->host_st->cond,
                              sizeof(unsigned long long), cudaMemcpyHostToDevice, s));
-    if (o.loop == CGX_LOOP_GRAPH) {
+    if (persist) {
+      CUDA_TRY(learned ? launch_learned_start(h) : jacobi_start());
+      CUDA_TRY(launch_inner_persist(h, sg, learned));
+      CUDA_TRY(outer_update(true));
+    } else if (graph_loop) {
       CUDA_TRY(cudaGraphLaunch(learned ? gl->exec : gj->exec, s));
     } else {
       if (learned) {
@@ -2425,12 +2520,11 @@ cgx_status build_sell(cgx_handle *h) {
   // The band copy when A's offsets fit it.
   Band plan;
   CGX_TRY(band_plan(h, plan));
-  // The slot map holds k * ld + i in an int.
-  if (plan.K > 0 && band_ld(h->N) * kBandMaxK <= (size_t)INT_MAX) {
+  // The slot map holds 4 i + k in an int.
+  if (plan.K > 0 && (size_t)h->N * kBandMaxK <= (size_t)INT_MAX) {
     const int N = h->N;
-    L->gb_ld = band_ld(N);
     Carver c;
-    size_t o_v = take_n<__nv_bfloat16>(c, L->gb_ld * kBandMaxK);
+    size_t o_v = take_n<__nv_bfloat16>(c, (size_t)N * kBandMaxK);
     size_t o_m = take_n<int>(c, (size_t)L->nnzL);
     CUDA_TRY(dev_alloc(h, (void **)&L->gb_mem, c.off));
     L->gb_val = (__nv_bfloat16 *)((char *)L->gb_mem + o_v);
@@ -2444,7 +2538,7 @@ cgx_status build_sell(cgx_handle *h) {
     CUDA_TRY(cudaMemsetAsync(L->gb_mem, 0, c.off, h->stream));
     CUDA_TRY(cudaMemsetAsync(h->flag, 0, sizeof(int), h->stream));
     k_gband_map<<<grid_stream(h, L->nnzL), kThreads, 0, h->stream>>>(
-        L->nnzL, L->grow, L->gcol, o, L->gb_ld, L->g2b, h->flag);
+        L->nnzL, L->grow, L->gcol, o, L->g2b, h->flag);
     CUDA_TRY(cudaGetLastError());
     int flag = 0;
     CUDA_TRY(cudaMemcpyAsync(&flag, h->flag, sizeof(int), cudaMemcpyDeviceToHost,
@@ -3024,7 +3118,7 @@ cgx_status cgx_solve(cgx_handle *h, const cgx_options *opts,
   if (o.preconditioner < CGX_PRECONDITIONER_NONE ||
       o.preconditioner > CGX_PRECONDITIONER_LEARNED ||
       o.precision < CGX_PRECISION_FP64 || o.precision > CGX_PRECISION_MIXED ||
-      o.loop < CGX_LOOP_GRAPH || o.loop > CGX_LOOP_KERNELS)
+      o.loop < CGX_LOOP_GRAPH || o.loop > CGX_LOOP_PERSISTENT)
     return fail(CGX_ERROR_INVALID_ARGUMENT, "invalid option value");
   if (o.preconditioner == CGX_PRECONDITIONER_LEARNED &&
       o.precision != CGX_PRECISION_MIXED)
@@ -3091,6 +3185,7 @@ cgx_status cgx_time_spmv(cgx_handle *h, cgx_precision precision, int reps,
   cudaStream_t s = h->stream;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
+  StencilGeom sg;
   CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
   cudaError_t e = cudaSuccess;
   for (int r = 0; r < reps && e == cudaSuccess; r++)
@@ -3098,7 +3193,7 @@ cgx_status cgx_time_spmv(cgx_handle *h, cgx_precision precision, int reps,
             ? launch_spmv(h, h->vec[CGX_VECTOR_P],
                           OpPcgQ{h->vec[CGX_VECTOR_P], h->vec[CGX_VECTOR_Q],
                                  ticket(h, kTicketQ)})
-            : h->band.ok ? launch_band_dir(h, 0, h->z32) : launch_inner_q(h);
+            : stencil_geom(h, &sg) ? launch_st_dir(h, sg, 0, h->z32) : launch_inner_q(h);
   const cudaError_t ec = cudaStreamEndCapture(s, &graph);
   if (e == cudaSuccess) e = ec;
   if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);

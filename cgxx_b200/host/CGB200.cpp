@@ -230,8 +230,10 @@ public:
         loop = CGX_LOOP_CHUNKED;
       else if (s == "kernels")
         loop = CGX_LOOP_KERNELS;
+      else if (s == "persistent")
+        loop = CGX_LOOP_PERSISTENT;
       else
-        badEnv("CG_B200_LOOP", "graph, chunked, or kernels");
+        badEnv("CG_B200_LOOP", "graph, chunked, kernels, or persistent");
     }
     if (const char *v = std::getenv("CG_B200_DEVICE"); v && *v) {
       char *end = nullptr;
@@ -282,7 +284,8 @@ public:
         printPadded("Learned set-up time:", std::to_string(learnedSetupSeconds));
       }
       static const char *loops[] = {"CUDA graph (while node)",
-                                    "CUDA graph chunks", "kernel launches"};
+                                    "CUDA graph chunks", "kernel launches",
+                                    "persistent inner solves"};
       printPadded("Device loop:", loops[loop]);
     }
   }

@@ -77,9 +77,15 @@ typedef enum cgx_precision {
 } cgx_precision;
 
 typedef enum cgx_loop {
-  CGX_LOOP_GRAPH = 0,   /* whole solve = one CUDA graph with a while node */
+  CGX_LOOP_GRAPH = 0,   /* whole solve = one CUDA graph with a while node;
+                           the mixed paths on a grid's band form switch to the
+                           persistent inner solve below where it is faster */
   CGX_LOOP_CHUNKED = 1, /* graph of a fixed number of iterations, host polls */
-  CGX_LOOP_KERNELS = 2  /* one launch per fused kernel, each timed by events */
+  CGX_LOOP_KERNELS = 2, /* one launch per fused kernel, each timed by events */
+  CGX_LOOP_PERSISTENT = 3 /* mixed paths on a grid's band form (the 7- and
+                           5-point stencils): each inner solve is one
+                           cooperative launch whose phases meet at grid-wide
+                           barriers; other solves run as GRAPH */
 } cgx_loop;
 
 /* Solver settings: the reference's CG_* environment switches

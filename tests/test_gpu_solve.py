@@ -305,6 +305,103 @@ def test_band_returns_after_an_asymmetric_refresh(handle):
     assert forms[2] == _expected_band(A)
 
 
+def _strided_band(N, seed):
+    """SPD matrix with offsets 0, +-2, +-9: a band form whose d_1 is not 1
+    (no lane shuffles)."""
+    rng = np.random.default_rng(seed)
+    rows, cols, vals = [np.arange(N)], [np.arange(N)], [np.full(N, 5.0)]
+    for off in (2, 9):
+        r = np.arange(N - off)
+        w = rng.uniform(0.2, 1.0, N - off)
+        rows += [r, r + off]
+        cols += [r + off, r]
+        vals += [-w, -w]
+    return G.crs_from_unsorted(N, np.concatenate(rows), np.concatenate(cols),
+                               np.concatenate(vals))
+
+
+@pytest.mark.parametrize("case", ["diffusion7_24", "diffusion7_37x23x11", "poisson2d_65",
+                                  "tridiagonal", "strided"])
+def test_band_loops_agree(handle, case):
+    """The mixed solve on the band forms in every loop mode: the grid
+    stencils (z-marching kernels, partial tiles for 37 x 23 x 11, the 2-D
+    form for the 5-point matrix; per-phase kernels in a graph, in chunks, one
+    launch at a time, and the persistent cooperative launch) and the generic
+    band kernels (tridiagonal, offsets 2 and 9, on which the persistent mode
+    runs as a graph). Every mode reaches the FP64 tolerance with inner
+    iteration counts within 2 % and the same solution."""
+    A = {"diffusion7_24": lambda: G.diffusion3d(24, 7, sigma=1.0, corr_len=8.0, seed=31),
+         "diffusion7_37x23x11": lambda: _grid7(37, 23, 11, seed=37),
+         "poisson2d_65": lambda: G.poisson2d(65),
+         "tridiagonal": lambda: _tridiagonal(20001, seed=32),
+         "strided": lambda: _strided_band(30011, seed=33)}[case]()
+    b, _ = G.rhs_for(A, seed=34)
+    handle.upload_crs(A.ptr, A.index, A.value)
+    handle.upload_jacobi(1.0 / A.diagonal())
+    handle.set_vector("K", b)
+    out = {}
+    for loop in (cg.LOOP_GRAPH, cg.LOOP_CHUNKED, cg.LOOP_KERNELS, cg.LOOP_PERSISTENT):
+        handle.fill_vector("X", 0.0)
+        r = handle.solve(max_iterations=50000, tolerance=1e-9, precision=cg.PRECISION_MIXED,
+                         loop=loop)
+        x = handle.get_vector("X")
+        assert r["converged"] == 1 and r["fell_back"] == 0, (loop, r)
+        assert np.linalg.norm(b - A.matvec(x)) / np.linalg.norm(b) <= 1e-9
+        out[loop] = (r, x)
+    assert handle.inner_band() == _expected_band(A)
+    rg, xg = out[cg.LOOP_GRAPH]
+    for loop in (cg.LOOP_CHUNKED, cg.LOOP_KERNELS, cg.LOOP_PERSISTENT):
+        rl, xl = out[loop]
+        assert abs(rl["iterations"] - rg["iterations"]) <= 0.02 * rg["iterations"] + 2
+        assert rel(xl, xg) <= 1e-6
+
+
+def _grid7(nx, ny, nz, seed):
+    """SPD 7-point matrix on an nx x ny x nz grid (x fastest)."""
+    rng = np.random.default_rng(seed)
+    N = nx * ny * nz
+    idx = np.arange(N).reshape(nz, ny, nx)
+    rows, cols, vals = [np.arange(N)], [np.arange(N)], [np.full(N, 7.0)]
+    for axis in (2, 1, 0):
+        a_ = idx.take(range(idx.shape[axis] - 1), axis=axis).ravel()
+        b_ = idx.take(range(1, idx.shape[axis]), axis=axis).ravel()
+        w = rng.uniform(0.2, 1.0, len(a_))
+        rows += [a_, b_]
+        cols += [b_, a_]
+        vals += [-w, -w]
+    return G.crs_from_unsorted(N, np.concatenate(rows), np.concatenate(cols),
+                               np.concatenate(vals))
+
+
+def test_learned_loops_agree(handle):
+    """The learned path (the fused stencil iteration on the 7-point band) in
+    the three loop modes: the same iterations within 2 % and solutions."""
+    from cgxx_b200 import learned as LRN
+    A = _grid7(41, 19, 13, seed=35)
+    b, _ = G.rhs_for(A, seed=36)
+    handle.upload_crs(A.ptr, A.index, A.value)
+    handle.upload_jacobi(1.0 / A.diagonal())
+    handle.set_vector("K", b)
+    handle.learned_setup()
+    net = cg.Gnn(0, LRN.load_weights(LRN.DEFAULT_WEIGHTS)[0])
+    handle.learned_factor(net, 1e-4)
+    net.close()
+    out = {}
+    for loop in (cg.LOOP_GRAPH, cg.LOOP_CHUNKED, cg.LOOP_KERNELS, cg.LOOP_PERSISTENT):
+        handle.fill_vector("X", 0.0)
+        r = handle.solve(max_iterations=20000, tolerance=1e-9, precision=cg.PRECISION_MIXED,
+                         preconditioner=cg.PRECOND_LEARNED, loop=loop)
+        x = handle.get_vector("X")
+        assert r["converged"] == 1 and r["fell_back"] == 0, (loop, r)
+        assert np.linalg.norm(b - A.matvec(x)) / np.linalg.norm(b) <= 1e-9
+        out[loop] = (r["iterations"], x)
+    ig, xg = out[cg.LOOP_GRAPH]
+    for loop in (cg.LOOP_CHUNKED, cg.LOOP_KERNELS, cg.LOOP_PERSISTENT):
+        il, xl = out[loop]
+        assert abs(il - ig) <= 0.02 * ig + 2, (loop, il, ig)
+        assert rel(xl, xg) <= 1e-6, loop
+
+
 def test_time_spmv_measures_the_fused_product(handle):
     """cgx_time_spmv times the solver's own SpMV (FP64 and the FP32 inner
     one) back to back, and a solve afterwards is unaffected."""
