@@ -495,14 +495,13 @@ def our_arm(args, world, rank, local):
         band = h.inner_band()
         prof_name = None  # ncu traffic is committed for the band form only
         if band:
-            # The fused first kernel of the band iteration: 4 FP32 values per
-            # row (diagonal and upper half, slot-major; the lower half is read
-            # from the rows above, in L1/L2), z and p_old read, d read and
-            # written, the new p and q written.
-            fp32_spmv_bytes = 16 * N + 4 * N + 4 * N + 8 * N + 4 * N + 4 * N
-            kname = (f"k_band_dir: p = z + b p_old, d += a p_old, q = A p, <p,q> "
-                     f"(FP32 symmetric band, offsets {band})")
-            prof_name = "spmv_band_dir_fp32_diffusion7_160.json"
+            # Symmetric band: 4 FP32 values per row (diagonal and upper half;
+            # the lower half is read from the rows above, in L1/L2), p once,
+            # q written.
+            fp32_spmv_bytes = 16 * N + 8 * N
+            kname = (f"k_band<4, OpInnerQ>: q = A p fused with <p,q> (FP32 symmetric band, "
+                     f"offsets {band})")
+            prof_name = "spmv_band_fp32_diffusion7_160.json"
         elif slots:
             # SELL-U: FP32 values, 16-byte slice descriptors, p once, q
             # written (a uniform slice carries no per-entry index).
@@ -561,18 +560,19 @@ def our_arm(args, world, rank, local):
 
     iters = res["iterations"]
     outer = res["outer_iterations"]
-    # The fused band iterations run two per graph body (the kernels of the
-    # iteration after a stop still launch and return at once).
-    fused = args.path != "plain" and bool(h.inner_band())
-    bodies = (iters + outer + 1) // 2
+    # Persistent inner solves (band form, up to 2.2M rows learned, 1.5M
+    # Jacobi): one cooperative launch per refinement step after its start.
+    persist = (args.path != "plain" and bool(h.inner_band())
+               and N <= (2200000 if args.path == "learned" else 1500000))
     if args.path == "plain":
         per_solve = 2 + 4 * iters                   # fill, set-up, 3 fused + guard
     elif args.path == "mixed":
-        # dot, true residuals, starts, updates, and per body 2 x 2 kernels + guard
-        per_solve = 2 + 3 * outer + 1 + (5 * bodies if fused else 4 * iters)
+        # dot, true residuals, start, update; per iteration 3 kernels + guard
+        per_solve = 2 + 3 * outer + 1 + (2 * outer if persist else 4 * iters)
     else:
-        # + set-up and network, and per body 2 x 3 kernels + guard
-        per_solve = 2 + 19 + 3 * outer + 1 + 3 * outer + (7 * bodies if fused else 7 * iters)
+        # + set-up and network; per iteration 5 kernels + guard + the
+        # start's apply (persistent: start, apply, one solve, update)
+        per_solve = 2 + 19 + 3 * outer + 1 + 3 * outer + (2 * outer if persist else 7 * iters)
     launches = args.steps * per_solve
 
     cpu = None

@@ -30,7 +30,6 @@
 #include "learned.cuh"
 #include "persist.cuh"
 #include "sell.cuh"
-#include "stencil.cuh"
 
 using namespace cgx;
 
@@ -204,8 +203,8 @@ struct cgx_handle {
   int16_t *idx16 = nullptr;
   bool compact16 = false;
   float *d32 = nullptr, *r32 = nullptr, *p32 = nullptr, *q32 = nullptr;
-  // Second buffers of the ping-pong pairs (p, r) and z of the fused band
-  // iterations (band.cuh).
+  // Second buffers of the ping-pong pairs (p, r) and z of the persistent
+  // inner solves (persist.cuh).
   float *p32b = nullptr, *r32b = nullptr, *z32 = nullptr;
   // Partial sums and the barrier counter of the persistent inner solves.
   double *persist_part = nullptr;
@@ -666,58 +665,6 @@ static cudaError_t launch_band(cgx_handle *h, const float *x, Op op) {
   return launch_rows(h, k_band<4, Op>, h->N, band_view(h), x, op, h->st, h->partials);
 }
 
-// The z-marching kernels are switched off until their loads are pipelined:
-// one plane at a time, each step waits a full memory latency (92 us for the
-// fused product at 160^3 against 31 us for the generic kernels).
-constexpr bool kStencilOn = false;
-
-// The z-marching kernels (stencil.cuh) apply when A is on the band and its
-// offsets are those of a 3-D (or 2-D) grid numbered x fastest: 0, 1, nx,
-// nx ny (or 0, 1, nx). The planes are cut into chunks so that the grid holds
-// about six CTAs per SM, and never more CTAs than the partial-sum slots.
-static bool stencil_geom(const cgx_handle *h, StencilGeom *g) {
-  if (!kStencilOn) return false;
-  const Band &B = h->band;
-  if (!B.ok || B.K < 3 || B.d[1] != 1 || B.d[2] < 2) return false;
-  const int nx = B.d[2];
-  long long plane;
-  if (B.K == 3) {
-    plane = h->N;
-  } else {
-    if (B.d[3] % nx != 0) return false;
-    plane = B.d[3];
-  }
-  if (plane % nx != 0 || h->N % plane != 0) return false;
-  g->nx = nx;
-  g->ny = (int)(plane / nx);
-  g->nz = (int)(h->N / plane);
-  g->tiles_x = (g->nx + kStX - 1) / kStX;
-  g->tiles_y = (g->ny + kStY - 1) / kStY;
-  const long long tiles = (long long)g->tiles_x * g->tiles_y;
-  if (tiles > kMaxGrid) return false;
-  const long long want = std::min<long long>(6LL * h->num_sms, kMaxGrid);
-  const int chunks = (int)std::max<long long>(
-      1, std::min<long long>({(long long)g->nz, (want + tiles - 1) / tiles, kMaxGrid / tiles}));
-  g->lz = (g->nz + chunks - 1) / chunks;
-  return true;
-}
-
-static int stencil_grid(const StencilGeom &g) {
-  return st_items(g);
-}
-
-// Step 1 of a fused band inner iteration (stencil.cuh): p from z and the
-// last p (buffer `parity`: 0 = p32, 1 = p32b) into the other buffer, the
-// lagged update of d, q = A p, a.
-static cudaError_t launch_st_dir(cgx_handle *h, const StencilGeom &g, int parity,
-                                 const float *z) {
-  const StDirArgs a{z, parity ? h->p32b : h->p32, parity ? h->p32 : h->p32b, h->d32,
-                    h->q32, ticket(h, kTicketInnerQ), parity ? 0 : 1};
-  k_st_dir<<<stencil_grid(g), kThreads, 0, h->stream>>>(g, band_view(h), a, h->st,
-                                                        h->partials);
-  return cudaGetLastError();
-}
-
 static cudaError_t launch_inner_q(cgx_handle *h) {
   OpInnerQ op{h->p32, h->q32, ticket(h, kTicketInnerQ)};
   if (h->band.ok) return launch_band(h, h->p32, op);
@@ -734,29 +681,11 @@ static cudaError_t launch_inner_q(cgx_handle *h) {
       h->p32, op);
 }
 
-// Inner FP32 PCG iteration of the mixed path. With A on the band of a grid
-// (stencil_geom) it is the fused two-kernel iteration of stencil.cuh on the
-// buffers of `parity`; its kernel-mode segments are (p update + q = A p |
-// r update | nothing).
-static cudaError_t launch_inner_iteration(cgx_handle *h, int parity,
-                                          cudaEvent_t *evs = nullptr) {
+// Inner FP32 PCG iteration of the mixed path: three kernels, whose
+// kernel-mode segments are (q = A p | r update | p update).
+static cudaError_t launch_inner_iteration(cgx_handle *h, cudaEvent_t *evs = nullptr) {
   cudaError_t e;
   const int g = grid_stream(h, (size_t)(h->N + 3) / 4);
-  StencilGeom sg;
-  if (stencil_geom(h, &sg)) {
-    if (evs) cudaEventRecord(evs[0], h->stream);
-    if ((e = launch_st_dir(h, sg, parity, h->z32)) != cudaSuccess) return e;
-    if (evs) cudaEventRecord(evs[1], h->stream);
-    k_inner_update<true><<<g, kThreads, 0, h->stream>>>(
-        h->N, h->r32, h->q32, h->C32, h->st, h->partials,
-        ticket(h, kTicketInnerUpdate), h->z32);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    if (evs) {
-      cudaEventRecord(evs[2], h->stream);
-      cudaEventRecord(evs[3], h->stream);
-    }
-    return cudaSuccess;
-  }
   if (evs) cudaEventRecord(evs[0], h->stream);
   e = launch_inner_q(h);
   if (e != cudaSuccess) return e;
@@ -2000,9 +1929,9 @@ static cudaError_t launch_learned_apply(cgx_handle *h, bool start) {
 
 // One inner solve as a persistent cooperative launch (persist.cuh), after
 // the path's start kernel(s). The grid is what the SMs hold at once, as a
-// cooperative launch requires (and no more CTAs than work items or
+// cooperative launch requires (and no more CTAs than 256-row tiles or
 // partial-sum slots).
-static cudaError_t launch_inner_persist(cgx_handle *h, const StencilGeom &g, bool learned) {
+static cudaError_t launch_inner_persist(cgx_handle *h, bool learned) {
   PersistArgs a;
   a.p[0] = h->p32;
   a.p[1] = h->p32b;
@@ -2019,27 +1948,41 @@ static cudaError_t launch_inner_persist(cgx_handle *h, const StencilGeom &g, boo
   BandView<4> A = band_view(h);
   GBandView G{};
   if (learned) G = gband_view(h);
-  StencilGeom gg = g;
-  void (*kern)(StencilGeom, BandView<4>, GBandView, PersistArgs, CgState *) =
+  void (*kern)(BandView<4>, GBandView, PersistArgs, CgState *) =
       learned ? k_inner_persist<true> : k_inner_persist<false>;
   int per_sm = 0;
   cudaError_t e =
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, 0);
   if (e != cudaSuccess) return e;
   if (per_sm < 1) return cudaErrorCooperativeLaunchTooLarge;
-  const int grid = std::max(1, std::min({h->num_sms * per_sm, kMaxGrid, st_items(g)}));
+  const long long tiles = ((long long)h->N + kThreads - 1) / kThreads;
+  const int grid = (int)std::max<long long>(
+      1, std::min<long long>({(long long)h->num_sms * per_sm, kMaxGrid, tiles}));
   e = cudaMemsetAsync(a.sync, 0, sizeof(unsigned long long), h->stream);
   if (e != cudaSuccess) return e;
   CgState *st = h->st;
-  void *args[] = {&gg, &A, &G, &a, &st};
+  void *args[] = {&A, &G, &a, &st};
   return cudaLaunchCooperativeKernel((const void *)kern, grid, kThreads, args, 0,
                                      h->stream);
 }
 
+// The persistent inner solve needs A on the band form (offsets 0 < d1 < d2
+// < d3, at most four), and for the learned path the factor on the band with
+// the same offsets.
+static bool persist_fits(const cgx_handle *h, bool learned) {
+  if (!h->band.ok || h->band.K > 4) return false;
+  if (!learned) return true;
+  if (!(h->L && h->L->gb_ok)) return false;
+  for (int k = 0; k < kBandMaxK; k++)
+    if (h->L->gb_d[k] != (k < h->band.K ? h->band.d[k] : 0)) return false;
+  return true;
+}
+
 // The default loop mode runs the persistent inner solve where it measured
-// faster than the graph of per-phase kernels: grids whose inner vectors and
-// values stay in L2 (up to 2M rows).
-static bool persist_pays(const cgx_handle *h) { return h->N <= (2 << 20); }
+// faster than the graph of per-phase kernels (kPersistMaxRows*).
+static bool persist_pays(const cgx_handle *h, bool learned) {
+  return h->N <= (learned ? kPersistMaxRows : kPersistMaxRowsJacobi);
+}
 
 static cudaError_t launch_learned_start(cgx_handle *h) {
   k_inner_start_z<<<grid_stream(h, h->N), kThreads, 0, h->stream>>>(
@@ -2050,42 +1993,10 @@ static cudaError_t launch_learned_start(cgx_handle *h) {
   return launch_learned_apply(h, true);
 }
 
-// Both A and G on the band of a grid: the learned inner iteration runs as
-// the fused three-kernel iteration of stencil.cuh.
-static bool learned_fused(const cgx_handle *h, StencilGeom *g) {
-  if (!(h->L && h->L->gb_ok) || !stencil_geom(h, g)) return false;
-  for (int k = 0; k < kBandMaxK; k++)
-    if (h->L->gb_d[k] != (k < h->band.K ? h->band.d[k] : 0)) return false;
-  return true;
-}
-
-// One learned inner iteration. Fused (learned_fused) on the buffers of
-// `parity`, with kernel-mode segments (p update + q = A p | r update +
-// y = G^T r | z = G y + eps C r); otherwise five kernels with segments
+// One learned inner iteration: five kernels, whose kernel-mode segments are
 // (q = A p | r update and the apply | p update).
-static cudaError_t launch_learned_iteration(cgx_handle *h, int parity,
-                                            cudaEvent_t *evs = nullptr) {
+static cudaError_t launch_learned_iteration(cgx_handle *h, cudaEvent_t *evs = nullptr) {
   cudaError_t e;
-  StencilGeom sg;
-  if (learned_fused(h, &sg)) {
-    Learned *L = h->L;
-    float *rold = parity ? h->r32b : h->r32, *rnew = parity ? h->r32 : h->r32b;
-    const int grid = stencil_grid(sg);
-    if (evs) cudaEventRecord(evs[0], h->stream);
-    if ((e = launch_st_dir(h, sg, parity, L->z32)) != cudaSuccess) return e;
-    if (evs) cudaEventRecord(evs[1], h->stream);
-    const StResArgs ra{rold, h->q32, rnew, L->y32, ticket(h, kTicketInnerUpdate)};
-    k_st_res<<<grid, kThreads, 0, h->stream>>>(sg, gband_view(h), ra, h->st, h->partials);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    if (evs) cudaEventRecord(evs[2], h->stream);
-    const OpLearnedZ zop{rnew, h->C32, L->z32, h->p32, L->eps, 0,
-                         ticket(h, kTicketInnerStart)};
-    k_st_gz<OpLearnedZ><<<grid, kThreads, 0, h->stream>>>(sg, gband_view(h), L->y32, zop,
-                                                           h->st, h->partials);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    if (evs) cudaEventRecord(evs[3], h->stream);
-    return cudaSuccess;
-  }
   if (evs) cudaEventRecord(evs[0], h->stream);
   e = launch_inner_q(h);
   if (e != cudaSuccess) return e;
@@ -2127,20 +2038,15 @@ static cgx_status solve_mixed(cgx_handle *h, const cgx_options &o,
   CUDA_TRY(cudaEventRecord(h->ev[6], s));
   CGX_TRY(ensure_f32(h));
 
-  // Fused band iterations (band.cuh) leave d's last update pending and
-  // alternate their ping-pong buffers, so a graph body runs two of them.
-  StencilGeom sg;
-  const bool fused_j = stencil_geom(h, &sg);
-  const bool fused_l = want_learned && learned_fused(h, &sg);
-  // The persistent inner solve (persist.cuh) on a grid's band form.
-  const bool persist = (want_learned ? fused_l : fused_j) &&
+  // The persistent inner solve (persist.cuh) leaves d's last update pending.
+  const bool persist = persist_fits(h, want_learned) &&
                        (o.loop == CGX_LOOP_PERSISTENT ||
-                        (o.loop == CGX_LOOP_GRAPH && persist_pays(h)));
-  // PERSISTENT on a matrix without a grid band form runs as GRAPH.
+                        (o.loop == CGX_LOOP_GRAPH && persist_pays(h, want_learned)));
+  // PERSISTENT on a matrix without the band form runs as GRAPH.
   const bool graph_loop =
       (o.loop == CGX_LOOP_GRAPH || o.loop == CGX_LOOP_PERSISTENT) && !persist;
-  auto outer_update = [&](bool pending) {
-    if (pending)
+  auto outer_update = [&] {
+    if (persist)
       k_outer_update_pending<<<grid_stream(h, h->N), kThreads, 0, h->stream>>>(
           h->N, h->vec[CGX_VECTOR_X], h->d32, h->p32, h->p32b, h->st);
     else
@@ -2155,33 +2061,28 @@ static cgx_status solve_mixed(cgx_handle *h, const cgx_options &o,
   auto jacobi_start = [&] {
     k_inner_start<<<grid_stream(h, h->N), kThreads, 0, h->stream>>>(
         h->N, h->r64, h->r32, h->d32, h->p32, h->C32, h->st, h->partials,
-        ticket(h, kTicketInnerStart), fused_j ? h->z32 : nullptr);
+        ticket(h, kTicketInnerStart), persist ? h->z32 : nullptr);
     return cudaGetLastError();
   };
   GraphEntry *gj = nullptr, *gl = nullptr;
   if (graph_loop) {
     CGX_TRY(build_while_graph(
-        h, fused_j ? 301 : 300, jacobi_start,
+        h, 300, jacobi_start,
         [&] {
-          cudaError_t e = launch_inner_iteration(h, 0);
-          if (e == cudaSuccess && fused_j) e = launch_inner_iteration(h, 1);
+          cudaError_t e = launch_inner_iteration(h);
           return e != cudaSuccess ? e : guard();
         },
-        [&] { return outer_update(fused_j); }, &gj));
+        outer_update, &gj));
     if (want_learned)
       CGX_TRY(build_while_graph(
-          h, fused_l ? 501 : 500, [&] { return launch_learned_start(h); },
+          h, 500, [&] { return launch_learned_start(h); },
           [&] {
-            cudaError_t e = launch_learned_iteration(h, 0);
-            if (e == cudaSuccess && fused_l) e = launch_learned_iteration(h, 1);
+            cudaError_t e = launch_learned_iteration(h);
             return e != cudaSuccess ? e : guard();
           },
-          [&] { return outer_update(fused_l); }, &gl));
+          outer_update, &gl));
   } else if (o.loop == CGX_LOOP_CHUNKED) {
-    int parity = 0;  // kChunk is even: every chunk starts at parity 0
-    CGX_TRY(build_chunk_graph(
-        h, fused_j ? 401 : 400,
-        [&] { return launch_inner_iteration(h, fused_j ? (parity++ & 1) : 0); }, &gj));
+    CGX_TRY(build_chunk_graph(h, 400, [&] { return launch_inner_iteration(h); }, &gj));
   }
   const unsigned long long cond_j = gj && graph_loop ? gj->cond : 0;
   const unsigned long long cond_l = gl ? gl->cond : 0;
@@ -2244,8 +2145,8 @@ static cgx_status solve_mixed(cgx_handle *h, const cgx_options &o,
                              sizeof(unsigned long long), cudaMemcpyHostToDevice, s));
     if (persist) {
       CUDA_TRY(learned ? launch_learned_start(h) : jacobi_start());
-      CUDA_TRY(launch_inner_persist(h, sg, learned));
-      CUDA_TRY(outer_update(true));
+      CUDA_TRY(launch_inner_persist(h, learned));
+      CUDA_TRY(outer_update());
     } else if (graph_loop) {
       CUDA_TRY(cudaGraphLaunch(learned ? gl->exec : gj->exec, s));
     } else {
@@ -2263,9 +2164,9 @@ static cgx_status solve_mixed(cgx_handle *h, const cgx_options &o,
         for (int c = 0; c < maxChunks; c++) {
           for (int j = 0; j < kChunk; j++) {
             if (learned)
-              CUDA_TRY(launch_learned_iteration(h, j & 1, &h->evpool[4 * j]));
+              CUDA_TRY(launch_learned_iteration(h, &h->evpool[4 * j]));
             else
-              CUDA_TRY(launch_inner_iteration(h, j & 1, &h->evpool[4 * j]));
+              CUDA_TRY(launch_inner_iteration(h, &h->evpool[4 * j]));
           }
           CGX_TRY(pull_state(h));
           const int now = h->host_st->total_inner;
@@ -2278,7 +2179,7 @@ static cgx_status solve_mixed(cgx_handle *h, const cgx_options &o,
         const int maxLaunches = o.max_iterations + 2;
         for (int l = 0; l < maxLaunches; l++) {
           if (learned)
-            CUDA_TRY(launch_learned_iteration(h, l & 1, nullptr));
+            CUDA_TRY(launch_learned_iteration(h, nullptr));
           else
             CUDA_TRY(cudaGraphLaunch(gj->exec, s));
           CUDA_TRY(cudaMemcpyAsync(h->host_scalar, &h->st->in_stop, sizeof(int),
@@ -2287,7 +2188,7 @@ static cgx_status solve_mixed(cgx_handle *h, const cgx_options &o,
           if (*(int *)h->host_scalar) break;
         }
       }
-      CUDA_TRY(outer_update(learned ? fused_l : fused_j));
+      CUDA_TRY(outer_update());
     }
   }
   CUDA_TRY(cudaEventRecord(h->ev[7], s));
@@ -3178,14 +3079,10 @@ cgx_status cgx_time_spmv(cgx_handle *h, cgx_precision precision, int reps,
   h->host_st->in_stop = 0;
   h->host_st->in_finished = 0;
   h->host_st->use_cond = 0;
-  // The fused band kernel's lagged updates start from a = b = 0.
-  h->host_st->in_alpha = 0.0;
-  h->host_st->in_beta = 0.0;
   CGX_TRY(push_state(h));
   cudaStream_t s = h->stream;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
-  StencilGeom sg;
   CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
   cudaError_t e = cudaSuccess;
   for (int r = 0; r < reps && e == cudaSuccess; r++)
@@ -3193,7 +3090,7 @@ cgx_status cgx_time_spmv(cgx_handle *h, cgx_precision precision, int reps,
             ? launch_spmv(h, h->vec[CGX_VECTOR_P],
                           OpPcgQ{h->vec[CGX_VECTOR_P], h->vec[CGX_VECTOR_Q],
                                  ticket(h, kTicketQ)})
-            : stencil_geom(h, &sg) ? launch_st_dir(h, sg, 0, h->z32) : launch_inner_q(h);
+            : launch_inner_q(h);
   const cudaError_t ec = cudaStreamEndCapture(s, &graph);
   if (e == cudaSuccess) e = ec;
   if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);

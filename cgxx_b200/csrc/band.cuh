@@ -11,14 +11,16 @@
 // instead of 28 (32 with SELL-U's padding), and the lower entries come from
 // rows the product read a moment earlier, which L1 and L2 still hold.
 //
-// The kernels here take any such offsets, one row per thread. When the
-// offsets are those of a 3-D grid numbered x fastest (1, nx, nx ny), the
-// z-marching kernels of stencil.cuh run instead: they read each row's
-// values once and take the neighbours from shared memory and registers.
-// Measured against these (160^3, back to back): a slot-major layout (every
-// load of a slot coalesced) and warp shuffles for the +-1 neighbours were
-// 4-40 % slower, because the products are bound by the latency of their
-// loads, not by sectors; one 16-byte load per row beats four 4-byte ones.
+// The kernels here take any such offsets, one row per thread. Measured
+// against them (160^3, back to back): a slot-major layout (every load of a
+// slot coalesced) and warp shuffles for the +-1 neighbours were 4-40 %
+// slower, because the products are bound by the latency of their loads, not
+// by sectors; one 16-byte load per row beats four 4-byte ones. Kernels that
+// march along z through a tile of x-y columns and take the neighbours from
+// shared memory (a register ring, or a four-stage asynchronous-copy
+// pipeline of planes) were 2-4 times slower still: each CTA streams a long
+// dependent sequence of planes, with too few loads in flight to cover HBM
+// latency.
 //
 // Wider sets are left to SELL-U. On the 27-point stencil (14 stored
 // offsets), row-major rows of 64 bytes spread each warp's lower-entry loads

@@ -1,16 +1,15 @@
-// Persistent inner solves of the mixed paths on a grid's band form.
+// Persistent inner solves of the mixed paths on the band form.
 //
 // Each inner FP32 PCG of a refinement step is one cooperative launch instead
-// of a graph of two or three kernels per iteration. The CTAs (all resident:
-// a cooperative launch guarantees it) loop over the work items of the
-// z-marching phases of the fused iteration (stencil.cuh) and meet at a
-// grid-wide barrier after each phase.
-// After a barrier every CTA adds the per-CTA partial sums of the phase in
-// the same fixed order, so all CTAs hold the same alpha, beta and residual
-// and take the same stop decision; no CTA waits for a last CTA to finish a
-// reduction, and no launch separates the phases. Vectors written inside the
-// launch are read back through L2 (st_ld<true>), never through the read-only
-// path, whose lines could be stale.
+// of a graph of four or five kernels per iteration. The CTAs (all resident:
+// a cooperative launch guarantees it) run the phases of the fused band
+// iteration (fused.cuh) over the rows and meet at a grid-wide barrier after
+// each phase. After a barrier every CTA adds the per-CTA partial sums of the
+// phase in the same fixed order, so all CTAs hold the same alpha, beta and
+// residual and take the same stop decision; no CTA waits for a last CTA to
+// finish a reduction, and no launch separates the phases. Vectors written
+// inside the launch are read back through L2 (__ldcg), never through the
+// read-only path, whose lines could be stale.
 //
 //   learned: A  p = z + b p_old, d += a_old p_old, q = A p       | <p,q> -> a
 //            B  r = r_old - a q, y = G^T r                        | <r,r> -> test
@@ -23,13 +22,29 @@
 // ends and the host reports CGX_ERROR_DEVICE.
 #pragma once
 
+#include "fused.cuh"
 #include "kernels.cuh"
-#include "stencil.cuh"
 
 namespace cgx {
 
 constexpr unsigned kSyncPolls = 1u << 24;
 enum : int { kErrGridSync = 4 };  // CgState::error: a grid barrier gave up
+
+// Largest systems the default loop mode solves with persistent inner
+// solves. The fused phases read p, z and r of neighbouring rows again, which
+// costs more as the vectors outgrow L2, and they save fewer launches on the
+// Jacobi path (two phases against five kernels for the learned one):
+// measured on the 7-point grids, learned 1.31x faster at 96^3 and 1.03x at
+// 128^3, Jacobi 1.31x faster at 96^3 and 1.08x slower at 128^3, both slower
+// at 160^3.
+#ifndef CGX_PERSIST_MAX_ROWS
+#define CGX_PERSIST_MAX_ROWS 2200000
+#endif
+#ifndef CGX_PERSIST_MAX_ROWS_JACOBI
+#define CGX_PERSIST_MAX_ROWS_JACOBI 1500000
+#endif
+constexpr int kPersistMaxRows = CGX_PERSIST_MAX_ROWS;
+constexpr int kPersistMaxRowsJacobi = CGX_PERSIST_MAX_ROWS_JACOBI;
 
 // Partial-sum slots: phase k of an iteration uses slot k, so a slot is
 // written again only two barriers after every CTA has read it.
@@ -53,7 +68,7 @@ __device__ __forceinline__ bool grid_sync(unsigned long long *count,
     __threadfence();
     atomicAdd(count, 1ull);
     unsigned i = 0;
-    while (ld_acquire_u64(count) < target && ++i < kSyncPolls) __nanosleep(64);
+    while (ld_acquire_u64(count) < target && ++i < kSyncPolls) __nanosleep(32);
     ok = i < kSyncPolls;
     __threadfence();
   }
@@ -88,24 +103,6 @@ __device__ __forceinline__ double sum_partials(const double *slot) {
   return tot;
 }
 
-// z = s + eps C r with <r,z>, reading r through L2 (it is written in
-// phase B of the same launch).
-struct ZRowL2 {
-  using Acc = Acc1;
-  const float *r, *C;
-  float *z;
-  float eps;
-  struct Pre {
-    float r, c;
-  };
-  __device__ Pre prefetch(int i) const { return Pre{__ldcg(r + i), __ldg(C + i)}; }
-  __device__ void row(int i, float s, Acc &a, const Pre &pr) const {
-    const float zi = fmaf(eps * pr.c, pr.r, s);
-    z[i] = zi;
-    a.a0 = fma((double)pr.r, (double)zi, a.a0);
-  }
-};
-
 struct PersistArgs {
   float *p[2];      // ping-pong search directions (slot 0 = the start's p)
   float *r[2];      // ping-pong residuals (slot 0 = the start's r)
@@ -138,13 +135,12 @@ __device__ __forceinline__ void persist_publish(CgState *st, double alpha, doubl
 
 template <bool LEARNED>
 __global__ void __launch_bounds__(kThreads)
-    k_inner_persist(StencilGeom g, BandView<4> A, GBandView G, PersistArgs a, CgState *st) {
+    k_inner_persist(BandView<4> A, GBandView G, PersistArgs a, CgState *st) {
   // Start state (k_inner_start / the learned start): p = z, a = b = 0.
   double rho = st->in_rho, alpha = st->in_alpha, beta = st->in_beta;
   const double nrm0 = st->in_nrm0, tol = st->in_tol;
   int total = st->total_inner;
   const int maxit = st->max_iter;
-  const int items = st_items(g);
   const unsigned long long nb = gridDim.x;
   unsigned long long bar = 0;
   double res = 0.0;
@@ -154,23 +150,18 @@ __global__ void __launch_bounds__(kThreads)
   for (;;) {
     // (selects, not a.p[par]: a runtime index would put the arrays in local memory)
     float *p_old = par ? a.p[1] : a.p[0], *p_new = par ? a.p[0] : a.p[1];
-    float *r_old = par ? a.r[1] : a.r[0], *r_new = par ? a.r[0] : a.r[1];
     // A: p, d, q = A p, <p,q>.
-    const StDirArgs da{a.z, p_old, p_new, a.d, a.q, nullptr, 1 - par};
-    double acc = 0.0;
-    for (int item = blockIdx.x; item < items; item += gridDim.x)
-      acc += st_dir_item<true>(g, A, da, (float)alpha, (float)beta, item);
-    put_partial(acc, slot0);
+    const DirArgs da{a.z, p_old, p_new, a.d, a.q};
+    put_partial(band_dir_rows(A, da, (float)alpha, (float)beta), slot0);
     if (!(ok = grid_sync(a.sync, ++bar * nb))) break;
     alpha = rho / sum_partials(slot0);
     // B: r and the residual test (learned: also y = G^T r; Jacobi: z, <r,z>).
-    double rr = 0.0, rz = 0.0;
     if (LEARNED) {
-      const StResArgs ra{r_old, a.q, r_new, a.y, nullptr};
-      for (int item = blockIdx.x; item < items; item += gridDim.x)
-        rr += st_res_item<true>(g, G, ra, (float)(-alpha), item);
-      put_partial(rr, slot1);
+      float *r_old = par ? a.r[1] : a.r[0], *r_new = par ? a.r[0] : a.r[1];
+      const ResArgs ra{r_old, a.q, r_new, a.y};
+      put_partial(gband_res_rows(G, ra, (float)(-alpha)), slot1);
     } else {
+      double rr, rz;
       inner_update_rows<true, true>(A.N, a.r[0], a.q, a.C, a.z, (float)(-alpha), rr, rz);
       put_partial(rr, slot1);
       put_partial(rz, slot2);
@@ -185,11 +176,8 @@ __global__ void __launch_bounds__(kThreads)
     if (stop) break;
     if (LEARNED) {
       // C: z = G y + eps C r, <r,z>.
-      Acc1 zacc;
-      const ZRowL2 zop{r_new, a.C, a.z, a.eps};
-      for (int item = blockIdx.x; item < items; item += gridDim.x)
-        st_gz_item<ZRowL2, true>(g, G, a.y, zop, zacc, item);
-      put_partial(zacc.a0, slot2);
+      const GzArgs za{a.y, par ? a.r[1] : a.r[0], a.C, a.z, a.eps};
+      put_partial(gband_z_rows(G, za), slot2);
       if (!(ok = grid_sync(a.sync, ++bar * nb))) break;
     }
     const double rzn = sum_partials(slot2);

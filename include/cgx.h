@@ -78,14 +78,15 @@ typedef enum cgx_precision {
 
 typedef enum cgx_loop {
   CGX_LOOP_GRAPH = 0,   /* whole solve = one CUDA graph with a while node;
-                           the mixed paths on a grid's band form switch to the
-                           persistent inner solve below where it is faster */
+                           the mixed paths on the band form switch to the
+                           persistent inner solve below where it is faster
+                           (learned: up to 2.2M rows; Jacobi: 1.5M) */
   CGX_LOOP_CHUNKED = 1, /* graph of a fixed number of iterations, host polls */
   CGX_LOOP_KERNELS = 2, /* one launch per fused kernel, each timed by events */
-  CGX_LOOP_PERSISTENT = 3 /* mixed paths on a grid's band form (the 7- and
-                           5-point stencils): each inner solve is one
-                           cooperative launch whose phases meet at grid-wide
-                           barriers; other solves run as GRAPH */
+  CGX_LOOP_PERSISTENT = 3 /* mixed paths on the band form (the 7- and
+                           5-point stencils, any size): each inner solve is
+                           one cooperative launch whose phases meet at
+                           grid-wide barriers; other solves run as GRAPH */
 } cgx_loop;
 
 /* Solver settings: the reference's CG_* environment switches
@@ -111,11 +112,9 @@ typedef struct cgx_result {
   int outer_iterations;  /* MIXED: refinement steps; 0 otherwise */
   double solve_ms;       /* device time of the solve (CUDA events) */
   /* CGX_LOOP_KERNELS only: device time per fused kernel class (ms) and the
-   * number of launches of each; zero in the other loop modes. FP64 and the
-   * unfused inner iterations: (q = A p | r update | p update). The fused
-   * inner iterations of the symmetric band form (see cgx_inner_band):
-   * spmv = p update + q = A p; update = r update (+ y = G^T r, learned);
-   * direction = z = G y + eps C r (learned) or 0 (Jacobi). */
+   * number of launches of each; zero in the other loop modes:
+   * (q = A p | r update, and for the learned path the apply z = G G^T r +
+   * eps C r | p update). */
   double spmv_ms, update_ms, direction_ms;
   int spmv_launches, update_launches, direction_launches;
   int fell_back;         /* MIXED: an FP32 refinement step broke down or
@@ -289,9 +288,8 @@ cgx_status cgx_true_residual(cgx_handle *h, double *rel);
 /* Device time of the solver's SpMV alone (no counterpart in the
  * reference): `reps` back-to-back launches of the fused product the solve
  * runs (FP64: q = A p with <p,q> on the uploaded format; MIXED: the FP32
- * inner q = A p with <p,q>, which on the symmetric band form is the fused
- * first kernel of the inner iteration, p = z + b p_old, d += a p_old,
- * q = A p, <p,q>) are captured into a CUDA graph and timed with CUDA events
+ * inner q = A p with <p,q> on the inner form) are captured into a CUDA
+ * graph and timed with CUDA events
  * on the handle's stream after one untimed launch of the graph;
  * *us_per_launch is the average. Uses the current P (FP64) or inner vectors
  * (MIXED) and overwrites Q, the inner vectors and the solver scalars of the

@@ -1,197 +1,98 @@
-"""The z-marching stencil kernels (cgxx_b200/csrc/stencil.cuh) restated in
-numpy (no GPU).
+"""The fused band row loops (cgxx_b200/csrc/fused.cuh) and the persistent
+inner solve built on them (cgxx_b200/csrc/persist.cuh), restated in numpy
+(no GPU).
 
-A CTA owns a 32 x 8 tile of the x-y plane (lane = x, warp = y) and marches
-through a chunk of planes; x and y neighbours come from a shared-memory tile
-with a one-cell halo, z neighbours from the previous and next plane of the
-thread's own column. Tiles may run past the grid's edge (their cells clamped
-to it). This file restates that arithmetic cell by cell and checks, before
-the kernels run on a device:
+One thread owns one row, grid-stride; row i's band values are the
+row-major U[i] (diagonal and upper entries at offsets 0 < d1 < d2 < d3) and
+its lower entries are read from the rows above, U[i - d_k][k]. The learned
+factor's band copy holds Gb[i][k] = G(i, i - d_k). Neighbour indices are
+clamped into [0, N - 1] before the load and the value masked afterwards.
+This file restates that arithmetic row by row and checks, before the
+kernels run on a device:
 
-  - every load stays inside the buffer it addresses (U and the factor hold
-    N rows, the vectors N + 8 entries) and every store hits a valid cell;
-  - the products equal A p, G y and G^T r (the symmetric band form's
-    values), on full and partial tiles, 2-D grids and uneven plane chunks;
-  - the fused inner iteration (p and r formed again at neighbouring cells,
-    ping-pong buffers, the lagged update of d applied at the end) gives
-    what the unfused PCG gives.
+  - every load stays inside the buffer it addresses (U, Gb and the vectors
+    hold N rows) on 3-D and 2-D grids, grids with fewer than four offsets,
+    and a band that is not a grid's;
+  - the products equal A p, G y and G^T r;
+  - the persistent loop (ping-pong p and r, d one update behind and applied
+    at the end, the learned and Jacobi phase orders) gives what the unfused
+    PCG gives;
+  - the partial-sum slots of the persistent phases are never rewritten
+    before every CTA has read them.
 """
 import numpy as np
 import pytest
 
 from cgxx_b200 import generators as G
 
-PAD = 8
-SX, SY = 32, 8
+f32 = np.float32
 
 
 class Buf:
     """A device buffer with bounds-checked loads."""
 
-    def __init__(self, values, size):
-        self.size = size
-        self.v = np.zeros((size,) + np.shape(values)[1:], np.float32)
+    def __init__(self, values, size=None):
+        values = np.asarray(values, np.float32)
+        self.size = len(values) if size is None else size
+        self.v = np.zeros((self.size,) + values.shape[1:], np.float32)
         self.v[:len(values)] = values
 
     def __getitem__(self, idx):
         idx = np.asarray(idx)
-        assert idx.min() >= 0 and idx.max() < self.size, (idx.min(), idx.max(), self.size)
+        if idx.size:
+            assert idx.min() >= 0 and idx.max() < self.size, (idx.min(), idx.max(), self.size)
         return self.v[idx]
 
 
-def geom(nx, ny, nz, sms=148):
-    tiles_x, tiles_y = -(-nx // SX), -(-ny // SY)
-    tiles = tiles_x * tiles_y
-    want = min(6 * sms, 1184)
-    chunks = max(1, min(nz, -(-want // tiles), 1184 // tiles))
-    lz = -(-nz // chunks)
-    return dict(nx=nx, ny=ny, nz=nz, tx=tiles_x, ty=tiles_y, lz=lz,
-                grid=tiles * -(-nz // lz))
+def fma(a, b, c):
+    return (np.float64(a) * np.asarray(b, np.float64) + np.asarray(c, np.float64)).astype(f32)
 
 
-def tiles_of(g):
-    """(tx, ty, z0, z1) per CTA, and the tile's clamped cell columns."""
-    lane, w = np.meshgrid(np.arange(SX), np.arange(SY))
-    lane, w = lane.ravel(), w.ravel()
-    for b in range(g["grid"]):
-        tx, rest = b % g["tx"], b // g["tx"]
-        ty, chunk = rest % g["ty"], rest // g["ty"]
-        x, y = tx * SX + lane, ty * SY + w
-        valid = (x < g["nx"]) & (y < g["ny"])
-        col = np.minimum(y, g["ny"] - 1) * g["nx"] + np.minimum(x, g["nx"] - 1)
-        z0 = chunk * g["lz"]
-        z1 = min(g["nz"], z0 + g["lz"])
-        yield lane, w, valid, col, z0, z1, x == g["nx"] - 1, y == g["ny"] - 1
+def band_dir(offs, U, z, pold, d, al, be, N):
+    """band_dir_rows: p = z + be p_old (own row and every neighbour the
+    product reads), d += al p_old, q = A p."""
+    i = np.arange(N)
+    nmax = N - 1
+    u = U[i]
+    po0 = pold[i]
+    p0 = fma(be, po0, z[i])
+    s = fma(u[:, 0], p0, np.zeros(N, f32))
+    for k in range(1, 4):
+        ju = np.minimum(i + offs[k], nmax)
+        s = fma(u[:, k], fma(be, pold[ju], z[ju]), s)
+    for k in range(1, 4):
+        j = i - offs[k]
+        jc = np.maximum(j, 0)
+        lv = np.where(j < 0, f32(0), U[jc][:, k])
+        s = fma(lv, fma(be, pold[jc], z[jc]), s)
+    dn = fma(al, po0, d[i])
+    return p0, dn, s
 
 
-def st_dir(g, U, z, pold, d, al, be, N):
-    """k_st_dir: returns (p_new, d_new, q) on the valid cells."""
-    plane = g["nx"] * g["ny"]
-    nx = g["nx"]
-    pn_out, d_out, q_out = np.full(N, np.nan), np.full(N, np.nan), np.full(N, np.nan)
-    pn = lambda j: be * pold[j] + z[j]  # noqa: E731
-    for lane, w, valid, col, z0, z1, _, _ in tiles_of(g):
-        if z0 >= z1:
-            continue
-        i = z0 * plane + col
-        p_m = pn(i - plane) if z0 > 0 else np.zeros(len(i))
-        lw = U[i - plane][:, 3] if z0 > 0 else np.zeros(len(i))
-        po_c = pold[i]
-        p_c = be * po_c + z[i]
-        for zz in range(z0, z1):
-            u = U[i]
-            inn = np.minimum(i + plane, N - 1)
-            po_n = pold[inn]
-            p_n = be * po_n + z[inn]
-            sp = np.zeros((SY + 2, SX + 2))
-            suy = np.zeros((SY, SX + 1))
-            suz = np.zeros((SY + 1, SX))
-            sp[w + 1, lane + 1] = p_c
-            suy[w, lane + 1] = u[:, 1]
-            suz[w + 1, lane] = u[:, 2]
-            m = lane == 0
-            sp[w[m] + 1, 0] = pn(np.maximum(i[m] - 1, 0))
-            suy[w[m], 0] = U[np.maximum(i[m] - 1, 0)][:, 1]
-            m = lane == SX - 1
-            sp[w[m] + 1, SX + 1] = pn(np.minimum(i[m] + 1, N - 1))
-            m = w == 0
-            sp[0, lane[m] + 1] = pn(np.maximum(i[m] - nx, 0))
-            suz[0, lane[m]] = U[np.maximum(i[m] - nx, 0)][:, 2]
-            m = w == SY - 1
-            sp[SY + 1, lane[m] + 1] = pn(np.minimum(i[m] + nx, N - 1))
-            lv1 = np.where(i < 1, 0, suy[w, lane])
-            lv2 = np.where(i < nx, 0, suz[w, lane])
-            lv3 = np.where(i < plane, 0, lw)
-            s = (u[:, 0] * p_c + u[:, 1] * sp[w + 1, lane + 2] + u[:, 2] * sp[w + 2, lane + 1]
-                 + u[:, 3] * p_n + lv1 * sp[w + 1, lane] + lv2 * sp[w, lane + 1] + lv3 * p_m)
-            iv = i[valid]
-            assert np.all(np.isnan(q_out[iv]))  # each cell written once
-            q_out[iv], pn_out[iv] = s[valid], p_c[valid]
-            d_out[iv] = d[iv] + al * po_c[valid]
-            p_m, p_c, po_c, lw = p_c, p_n, po_n, u[:, 3]
-            i = i + plane
-    return pn_out, d_out, q_out
+def gband_res(offs, Gb, rold, q, na, N):
+    """gband_res_rows: r = r_old + na q (own row and the rows below it that
+    G^T reads), y = G^T r."""
+    i = np.arange(N)
+    r0 = fma(na, q[i], rold[i])
+    s = fma(Gb[i][:, 0], r0, np.zeros(N, f32))
+    for k in range(1, 4):
+        j = i + offs[k]
+        jc = np.minimum(j, N - 1)
+        v = np.where(j < N, Gb[jc][:, k], f32(0))
+        s = fma(v, fma(na, q[jc], rold[jc]), s)
+    return r0, s
 
 
-def st_res(g, Gb, rold, q, al, N):
-    """k_st_res: returns (r_new, y = G^T r_new)."""
-    plane, nx = g["nx"] * g["ny"], g["nx"]
-    r_out, y_out = np.full(N, np.nan), np.full(N, np.nan)
-    rn = lambda j: rold[j] - al * q[j]  # noqa: E731
-    for lane, w, valid, col, z0, z1, xlast, ylast in tiles_of(g):
-        if z0 >= z1:
-            continue
-        i = z0 * plane + col
-        r_c, gc = rn(i), Gb[i]
-        for zz in range(z0, z1):
-            inn = np.minimum(i + plane, N - 1)
-            r_n, gn = rn(inn), Gb[inn]
-            sr = np.zeros((SY + 1, SX + 1))
-            sg1 = np.zeros((SY, SX + 1))
-            sg2 = np.zeros((SY + 1, SX))
-            sr[w, lane], sg1[w, lane], sg2[w, lane] = r_c, gc[:, 1], gc[:, 2]
-            m = lane == SX - 1
-            j = np.minimum(i[m] + 1, N - 1)
-            sr[w[m], SX], sg1[w[m], SX] = rn(j), Gb[j][:, 1]
-            m = w == SY - 1
-            j = np.minimum(i[m] + nx, N - 1)
-            sr[SY, lane[m]], sg2[SY, lane[m]] = rn(j), Gb[j][:, 2]
-            v1 = np.where((i + 1 < N) & ~xlast, sg1[w, lane + 1], 0)
-            v2 = np.where((i + nx < N) & ~ylast, sg2[w + 1, lane], 0)
-            v3 = np.where(i + plane < N, gn[:, 3], 0)
-            s = gc[:, 0] * r_c + v1 * sr[w, lane + 1] + v2 * sr[w + 1, lane] + v3 * r_n
-            iv = i[valid]
-            assert np.all(np.isnan(y_out[iv]))
-            r_out[iv], y_out[iv] = r_c[valid], s[valid]
-            r_c, gc = r_n, gn
-            i = i + plane
-    return r_out, y_out
-
-
-def st_gz(g, Gb, y, N):
-    """k_st_gz: z = G y."""
-    plane, nx = g["nx"] * g["ny"], g["nx"]
-    out = np.full(N, np.nan)
-    for lane, w, valid, col, z0, z1, _, _ in tiles_of(g):
-        if z0 >= z1:
-            continue
-        i = z0 * plane + col
-        y_m = y[i - plane] if z0 > 0 else y[np.zeros(len(i), int)]
-        y_c = y[i]
-        for zz in range(z0, z1):
-            gv = Gb[i]
-            sy = np.zeros((SY + 1, SX + 1))
-            sy[w + 1, lane + 1] = y_c
-            m = lane == 0
-            sy[w[m] + 1, 0] = y[np.maximum(i[m] - 1, 0)]
-            m = w == 0
-            sy[0, lane[m] + 1] = y[np.maximum(i[m] - nx, 0)]
-            y_n = y[np.minimum(i + plane, N - 1)]
-            s = (gv[:, 0] * y_c + gv[:, 1] * sy[w + 1, lane] + gv[:, 2] * sy[w, lane + 1]
-                 + gv[:, 3] * y_m)
-            iv = i[valid]
-            assert np.all(np.isnan(out[iv]))
-            out[iv] = s[valid]
-            y_m, y_c = y_c, y_n
-            i = i + plane
-    return out
-
-
-def band_rows(A, nx, plane):
-    """Row-major U (N x 4) for offsets 0, 1, nx, plane and the lower factor
-    values Gb[i][k] = G(i, i - d_k) of G = |tril(A)| scaled."""
-    d = [0, 1, nx, plane]
-    rows = np.repeat(np.arange(A.N), np.diff(A.ptr))
-    U = np.zeros((A.N, 4), np.float32)
-    Gb = np.zeros((A.N, 4), np.float32)
-    top = np.abs(A.value).max()
-    for r, c, v in zip(rows, A.index, A.value):
-        if c >= r:
-            U[r, d.index(int(c - r))] = v
-        else:
-            Gb[r, d.index(int(r - c))] = abs(v) / top
-    Gb[np.arange(A.N), 0] = 1.0
-    return U, Gb
+def gband_z(offs, Gb, y, r, C, eps, N):
+    """gband_z_rows: z = G y + eps C r (the factor's band holds 0 where
+    i - d_k < 0)."""
+    i = np.arange(N)
+    g = Gb[i]
+    s = np.zeros(N, f32)
+    for k in range(4):
+        s = fma(g[:, k], y[np.maximum(i - offs[k], 0)], s)
+    ri = r[i]
+    return fma((f32(eps) * C[i]).astype(f32), ri, s)
 
 
 def grid_matrix(nx, ny, nz, seed):
@@ -213,22 +114,45 @@ def grid_matrix(nx, ny, nz, seed):
                                np.concatenate(vals))
 
 
-CASES = {"full": (64, 16, 5), "partial": (37, 11, 7), "chunked": (9, 9, 41),
-         "flat": (45, 20, 1), "thin": (33, 3, 2)}
+def odd_band_matrix(N, offs, seed):
+    """SPD matrix whose offsets are `offs` (not a grid's)."""
+    rng = np.random.default_rng(seed)
+    rows, cols, vals = [np.arange(N)], [np.arange(N)], [np.full(N, 2.0 * len(offs) + 1)]
+    for dk in offs[1:]:
+        a = np.arange(N - dk)
+        wv = rng.uniform(0.2, 1.0, len(a))
+        rows += [a, a + dk]
+        cols += [a + dk, a]
+        vals += [-wv, -wv]
+    return G.crs_from_unsorted(N, np.concatenate(rows), np.concatenate(cols),
+                               np.concatenate(vals))
 
 
-def _setup(case):
-    nx, ny, nz = CASES[case]
-    A = grid_matrix(nx, ny, nz, seed=nx + ny + nz)
-    U, Gb = band_rows(A, nx, nx * ny)
-    g = geom(nx, ny, nz)
-    return A, U, Gb, g
+def band_rows(A, offs):
+    """Row-major U (N x 4) and the factor's band Gb (N x 4) of G = the
+    scaled |tril(A)| with unit diagonal; offsets past the stored ones are 0
+    with zero values, as the device views pad them."""
+    rows = np.repeat(np.arange(A.N), np.diff(A.ptr))
+    U = np.zeros((A.N, 4), np.float32)
+    Gb = np.zeros((A.N, 4), np.float32)
+    top = np.abs(A.value).max()
+    for r, c, v in zip(rows, A.index, A.value):
+        if c >= r:
+            U[r, offs.index(int(c - r))] = v
+        else:
+            Gb[r, offs.index(int(r - c))] = abs(v) / top
+    Gb[np.arange(A.N), 0] = 1.0
+    return U, Gb, list(offs) + [0] * (4 - len(offs))
 
 
-def _lower_csr(Gb, nx, plane):
+def lower_csr(Gb, offs):
+    """G and G^T as CRS from the factor's band (the padded offsets, 0 with
+    zero values, add nothing)."""
     N = len(Gb)
     rows, cols, vals = [], [], []
-    for k, dk in enumerate((0, 1, nx, plane)):
+    for k, dk in enumerate(offs):
+        if k > 0 and dk == 0:
+            continue
         r = np.arange(N)
         keep = (Gb[:, k] != 0) & (r - dk >= 0)
         rows.append(r[keep])
@@ -238,68 +162,152 @@ def _lower_csr(Gb, nx, plane):
     return (G.crs_from_unsorted(N, rows, cols, vals), G.crs_from_unsorted(N, cols, rows, vals))
 
 
+CASES = {"grid3d": (23, 11, 7), "grid2d": (45, 20, 1), "thin": (33, 3, 2),
+         "line": (1, 1, 17), "odd": None}
+
+
+def _setup(case):
+    if case == "odd":
+        offs = [0, 1, 5, 19]
+        A = odd_band_matrix(301, offs, seed=3)
+    else:
+        nx, ny, nz = CASES[case]
+        A = grid_matrix(nx, ny, nz, seed=nx + ny + nz)
+        offs = [0]
+        # the offsets a neighbour pair really has: x (nx > 1), y (ny > 1), z (nz > 1)
+        for dk, present in ((1, nx > 1), (nx, ny > 1), (nx * ny, nz > 1)):
+            if present and dk not in offs:
+                offs.append(dk)
+        offs.sort()
+    U, Gb, d4 = band_rows(A, offs)
+    return A, U, Gb, d4
+
+
 @pytest.mark.parametrize("case", sorted(CASES))
-def test_stencil_products_stay_in_bounds_and_match(case):
-    A, U, Gb, g = _setup(case)
+def test_fused_products_stay_in_bounds_and_match(case):
+    A, U, Gb, d4 = _setup(case)
     N = A.N
     rng = np.random.default_rng(1)
-    size = N + PAD
-    x = Buf(rng.standard_normal(N).astype(np.float32), size)
-    zero = Buf(np.zeros(N, np.float32), size)
-    pn, dn, q = st_dir(g, Buf(U, N), x, zero, zero, 0.0, 0.0, N)
+    x = Buf(rng.standard_normal(N))
+    zero = Buf(np.zeros(N))
+    pn, dn, q = band_dir(d4, Buf(U), x, zero, zero, 0.0, 0.0, N)
     A32 = G.Crs(N, A.ptr, A.index, A.value.astype(np.float32).astype(np.float64))
-    xd = x.v[:N].astype(np.float64)
+    xd = x.v.astype(np.float64)
     assert np.allclose(q, A32.matvec(xd), rtol=1e-5, atol=1e-5)
-    assert np.array_equal(pn, x.v[:N]) and np.all(dn == 0)
-    Gl, Gt = _lower_csr(Gb, g["nx"], g["nx"] * g["ny"])
-    assert np.allclose(st_gz(g, Buf(Gb, N), x, N), Gl.matvec(xd), rtol=1e-5, atol=1e-5)
-    rn, y = st_res(g, Buf(Gb, N), x, zero, 0.0, N)
-    assert np.array_equal(rn, x.v[:N])
+    assert np.array_equal(pn, x.v) and np.all(dn == 0)
+    Gl, Gt = lower_csr(Gb, d4)
+    C = Buf(rng.uniform(0.5, 1.5, N))
+    zg = gband_z(d4, Buf(Gb), x, zero, C, 0.0, N)
+    assert np.allclose(zg, Gl.matvec(xd), rtol=1e-5, atol=1e-5)
+    rn, y = gband_res(d4, Buf(Gb), x, zero, 0.0, N)
+    assert np.array_equal(rn, x.v)
     assert np.allclose(y, Gt.matvec(xd), rtol=1e-5, atol=1e-5)
 
 
-@pytest.mark.parametrize("case", ["partial", "chunked", "flat"])
-def test_fused_learned_iteration_matches_pcg(case):
-    """Inner PCG with M^-1 = G G^T: the fused stencil kernels (ping-pong p
-    and r, d one update behind, applied at the end) against a plain PCG."""
-    A, U, Gb, g = _setup(case)
-    N = A.N
-    Gl, Gt = _lower_csr(Gb, g["nx"], g["nx"] * g["ny"])
-    A32 = G.Crs(N, A.ptr, A.index, A.value.astype(np.float32).astype(np.float64))
-    b = np.random.default_rng(6).standard_normal(N)
-    iters = 12
-
-    xr, r = np.zeros(N), b.copy()
-    zz = Gl.matvec(Gt.matvec(r))
+def _pcg(A32, apply, b, iters):
+    xr, r = np.zeros(len(b)), b.copy()
+    zz = apply(r)
     p, rho = zz.copy(), r @ zz
     for _ in range(iters):
         q = A32.matvec(p)
         a = rho / (p @ q)
         xr += a * p
         r -= a * q
-        zz = Gl.matvec(Gt.matvec(r))
+        zz = apply(r)
         rn = r @ zz
         p = zz + (rn / rho) * p
         rho = rn
+    return xr
 
-    size = N + PAD
-    Ub, Gbb = Buf(U, N), Buf(Gb, N)
-    rbuf = [Buf(b.astype(np.float32), size), Buf(np.zeros(N, np.float32), size)]
-    zv = Buf(Gl.matvec(Gt.matvec(rbuf[0].v[:N].astype(np.float64))).astype(np.float32), size)
-    pbuf = [Buf(zv.v[:N], size), Buf(np.zeros(N, np.float32), size)]
-    dv = Buf(np.zeros(N, np.float32), size)
-    rho = float(rbuf[0].v[:N].astype(np.float64) @ zv.v[:N])
+
+@pytest.mark.parametrize("learned", [True, False])
+@pytest.mark.parametrize("case", ["grid3d", "grid2d", "odd"])
+def test_persistent_iteration_matches_pcg(case, learned):
+    """k_inner_persist's phases in its order (ping-pong p and r, d one
+    update behind, applied at the end as k_outer_update_pending does)
+    against a plain PCG with M^-1 = G G^T + eps C or C."""
+    A, U, Gb, d4 = _setup(case)
+    N = A.N
+    Gl, Gt = lower_csr(Gb, d4)
+    A32 = G.Crs(N, A.ptr, A.index, A.value.astype(np.float32).astype(np.float64))
+    rng = np.random.default_rng(6)
+    b = rng.standard_normal(N)
+    Cv = rng.uniform(0.5, 1.5, N).astype(np.float32)
+    eps = 0.25 if learned else 0.0
+    iters = 12
+    if learned:
+        apply = lambda r: Gl.matvec(Gt.matvec(r)) + eps * Cv * r
+    else:
+        apply = lambda r: Cv * r
+    xr = _pcg(A32, apply, b, iters)
+
+    Ub, Gbb, C = Buf(U), Buf(Gb), Buf(Cv)
+    r = [Buf(b), Buf(np.zeros(N))]
+    z = Buf(apply(r[0].v.astype(np.float64)))
+    p = [Buf(z.v), Buf(np.zeros(N))]
+    d = Buf(np.zeros(N))
+    rho = float(r[0].v.astype(np.float64) @ z.v)
     al = be = 0.0
-    for it in range(iters):
-        par = it & 1
-        pn, dn, q = st_dir(g, Ub, zv, pbuf[par], dv, al, be, N)
-        pbuf[1 - par], dv, qb = Buf(pn, size), Buf(dn, size), Buf(q, size)
-        al = rho / float(pn @ q)
-        rnew, y = st_res(g, Gbb, rbuf[par], qb, al, N)
-        rbuf[1 - par] = Buf(rnew, size)
-        zvv = st_gz(g, Gbb, Buf(y, size), N)
-        zv = Buf(zvv, size)
-        rn = float(rnew.astype(np.float64) @ zvv)
+    par = 0
+    for _ in range(iters):
+        pn, dn, q = band_dir(d4, Ub, z, p[par], d, al, be, N)
+        p[1 - par], d, qb = Buf(pn), Buf(dn), Buf(q)
+        al = rho / float(pn.astype(np.float64) @ q)
+        if learned:
+            rn_, y = gband_res(d4, Gbb, r[par], qb, -al, N)
+            r[1 - par] = Buf(rn_)
+        else:
+            r0 = fma(-al, q, r[0].v)
+            r[0] = Buf(r0)
+            z = Buf(Cv * r0)
+        par = 1 - par
+        if learned:
+            rcur = r[par]
+            z = Buf(gband_z(d4, Gbb, Buf(y), rcur, C, eps, N))
+        else:
+            rcur = r[0]
+        rn = float(rcur.v.astype(np.float64) @ z.v)
         be, rho = rn / rho, rn
-    xf = dv.v[:N] + al * pbuf[iters & 1].v[:N]
+    xf = d.v + al * p[par].v
     assert np.allclose(xf, xr, rtol=2e-3, atol=2e-3 * np.abs(xr).max())
+
+
+@pytest.mark.parametrize("learned", [True, False])
+def test_persistent_slots_are_read_before_reuse(learned):
+    """Phase k writes slot k before a barrier and every CTA reads it after
+    that barrier (the Jacobi phase B writes slots 1 and 2, read after its
+    barrier). A CTA may write a slot again only once it has passed a later
+    barrier than the one after which the slot was last read: then every CTA
+    has finished reading it."""
+    bar = 0
+    last_read = {}  # slot -> barrier after which it was read
+    for it in range(5):
+        events = [("w", 0), ("b",), ("r", 0)]
+        if learned:
+            events += [("w", 1), ("b",), ("r", 1), ("w", 2), ("b",), ("r", 2)]
+        else:
+            events += [("w", 1), ("w", 2), ("b",), ("r", 1), ("r", 2)]
+        for e in events:
+            if e[0] == "b":
+                bar += 1
+            elif e[0] == "r":
+                last_read[e[1]] = bar
+            else:
+                assert e[1] not in last_read or bar > last_read[e[1]], (it, e, bar, last_read)
+
+
+def test_persistent_grid_fits_the_slots():
+    """The persistent grid (SMs x resident CTAs, at most one CTA per 256-row
+    tile) never exceeds the kMaxGrid partial-sum slots, and the grid-stride
+    row loops cover every row once."""
+    kMaxGrid, kThreads = 148 * 8, 256
+    for per_sm in (1, 4, 5, 8):
+        for N in (1, 255, 256, 257, 884736, 2200000):
+            tiles = -(-N // kThreads)
+            grid = max(1, min(148 * per_sm, kMaxGrid, tiles))
+            assert grid <= kMaxGrid
+            seen = np.zeros(N, np.int32)
+            for blk in range(grid):
+                for start in range(blk * kThreads, N, grid * kThreads):
+                    seen[start:min(N, start + kThreads)] += 1
+            assert np.all(seen == 1)
