@@ -306,6 +306,51 @@ def _read_profile(name):
         return None
 
 
+# Algorithmic bytes per row of one inner iteration of the persistent inner
+# solves (persist.cuh), full and for the last iteration of a launch (which
+# stops after its residual test): FP32 vectors 4 bytes, U 16, the factor 8.
+#   split learned: q=Ap 24 | r, d 24 | y=G^T r 16 | z 24 | p 12
+#   split Jacobi:  q=Ap 24 | r, d, <r,Cr> 28 | p = C r + b p 16
+#   fused learned: p, d, q 40 | r, y 24 | z 24
+#   fused Jacobi:  p, d, q 40 | r, z 20
+PERSIST_BYTES = {(2, True): (100, 48), (2, False): (68, 52),
+                 (1, True): (88, 64), (1, False): (60, 60)}
+PERSIST_KERNEL = {(2, True): "k_inner_persist_split<learned>", (2, False): "k_inner_persist_split<Jacobi>",
+                  (1, True): "k_inner_persist<learned>", (1, False): "k_inner_persist<Jacobi>"}
+
+
+def persist_roofline(args, results, N, peak, peak_kind):
+    """Roofline of the persistent inner-solve launches of the timed solves:
+    their algorithmic bytes over their device time (CUDA events around each
+    launch, recorded by the library on its stream)."""
+    if args.path == "plain" or not results or results[-1]["inner_form"] == 0:
+        return None
+    form = results[-1]["inner_form"]
+    full, last = PERSIST_BYTES[(form, args.path == "learned")]
+    bytes_, ms, launches, its = 0, 0.0, 0, 0
+    for r in results:
+        if r["fell_back"] or r["inner_launches"] == 0:
+            continue
+        bytes_ += (r["iterations"] * full - r["inner_launches"] * (full - last)) * N
+        ms += r["inner_ms"]
+        launches += r["inner_launches"]
+        its += r["iterations"]
+    if launches == 0 or ms <= 0:
+        return None
+    key = (form, args.path == "learned")
+    out = {"bound": "hbm", "achieved": bytes_ / (ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+           "kernel": PERSIST_KERNEL[key] + ": one inner solve per launch",
+           "launch_us": 1e3 * ms / launches, "launches": launches,
+           "iterations_per_launch": its / launches,
+           "algorithmic_bytes": bytes_ / launches, "peak_kind": peak_kind}
+    out["frac"] = out["achieved"] / peak
+    prof = read_traffic_profile(f"persist_{'split' if form == 2 else 'fused'}_"
+                                f"{args.path}_diffusion7_160.json", args)
+    per_it = prof.get("dram_bytes_per_iteration") if prof else None
+    out["traffic"] = per_it * its / launches if per_it else None
+    return out
+
+
 def peaks():
     p = os.path.join(REPO, "MEASURED_PEAKS.json")
     try:
@@ -487,9 +532,8 @@ def our_arm(args, world, rank, local):
     fp64_roof["frac"] = fp64_roof["achieved"] / peak
     prof = read_traffic_profile("spmv_crs_fp64_diffusion7_160.json", args)
     fp64_roof["traffic"] = prof.get("dram_bytes_per_launch") if prof else None
-    if args.path == "plain":
-        roof = fp64_roof
-    else:
+    inner_roof = None
+    if args.path != "plain":
         kk = kern[args.path]
         slots, uniform, slices = h.inner_layout()
         band = h.inner_band()
@@ -510,13 +554,17 @@ def our_arm(args, world, rank, local):
                      f"{uniform}/{slices} slices uniform, {slots} value slots)")
         else:
             kname = "k_crs<float, OpInnerQ>: q = A p fused with <p,q> (FP32 CRS, inner)"
-        roof = {"bound": "hbm", "achieved": fp32_spmv_bytes / (spmv_us[args.path] * 1e-6) / 1e9,
-                "launch_us": spmv_us[args.path],
-                "peak": peak, "unit": "GB/s", "kernel": kname,
-                "algorithmic_bytes": fp32_spmv_bytes, "peak_kind": peak_kind}
-        roof["frac"] = roof["achieved"] / peak
+        inner_roof = {"bound": "hbm", "achieved": fp32_spmv_bytes / (spmv_us[args.path] * 1e-6) / 1e9,
+                      "launch_us": spmv_us[args.path],
+                      "peak": peak, "unit": "GB/s", "kernel": kname,
+                      "algorithmic_bytes": fp32_spmv_bytes, "peak_kind": peak_kind}
+        inner_roof["frac"] = inner_roof["achieved"] / peak
         prof32 = read_traffic_profile(prof_name, args) if prof_name else None
-        roof["traffic"] = prof32.get("dram_bytes_per_launch") if prof32 else None
+        inner_roof["traffic"] = prof32.get("dram_bytes_per_launch") if prof32 else None
+    roof = fp64_roof if args.path == "plain" else inner_roof
+    persist = persist_roofline(args, results, N, peak, peak_kind)
+    if persist is not None:
+        roof = persist
 
     # End to end through the public C ABI: pinned host inputs uploaded every
     # step (matrix, Jacobi C, right-hand side), the learned set-up and
@@ -560,10 +608,9 @@ def our_arm(args, world, rank, local):
 
     iters = res["iterations"]
     outer = res["outer_iterations"]
-    # Persistent inner solves (band form, up to 2.2M rows learned, 1.5M
-    # Jacobi): one cooperative launch per refinement step after its start.
-    persist = (args.path != "plain" and bool(h.inner_band())
-               and N <= (2200000 if args.path == "learned" else 1500000))
+    # Persistent inner solves: one cooperative launch per refinement step
+    # after its start.
+    persist = args.path != "plain" and res["inner_form"] != 0
     if args.path == "plain":
         per_solve = 2 + 4 * iters                   # fill, set-up, 3 fused + guard
     elif args.path == "mixed":
@@ -597,6 +644,7 @@ def our_arm(args, world, rank, local):
             "plain_iteration_gbs": plain_iter_bytes / (plain_iter_us * 1e-6) / 1e9,
             "plain_iteration_frac": plain_iter_bytes / (plain_iter_us * 1e-6) / 1e9 / peak,
             "roofline": roof,
+            "roofline_inner_spmv": inner_roof,
             "roofline_fp64_spmv": fp64_roof,
             "clocks": clocks,
             "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": h2d,

@@ -14,6 +14,6 @@ from ._lib import (  # noqa: F401
     FORMAT_COO, FORMAT_CRS, FORMAT_ELL,
     PRECOND_NONE, PRECOND_JACOBI, PRECOND_LEARNED,
     PRECISION_FP64, PRECISION_MIXED,
-    LOOP_GRAPH, LOOP_CHUNKED, LOOP_KERNELS, LOOP_PERSISTENT,
+    LOOP_GRAPH, LOOP_CHUNKED, LOOP_KERNELS, LOOP_PERSISTENT, LOOP_PERSISTENT_SPLIT,
     VECTOR_K, VECTOR_X, VECTOR_P, VECTOR_Q, VECTOR_R, VECTOR_Z,
 )

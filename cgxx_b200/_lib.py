@@ -24,7 +24,7 @@ VECTORS = {"K": 0, "X": 1, "P": 2, "Q": 3, "R": 4, "Z": 5}
 FORMAT_COO, FORMAT_CRS, FORMAT_ELL = range(3)
 PRECOND_NONE, PRECOND_JACOBI, PRECOND_LEARNED = range(3)
 PRECISION_FP64, PRECISION_MIXED = range(2)
-LOOP_GRAPH, LOOP_CHUNKED, LOOP_KERNELS, LOOP_PERSISTENT = range(4)
+LOOP_GRAPH, LOOP_CHUNKED, LOOP_KERNELS, LOOP_PERSISTENT, LOOP_PERSISTENT_SPLIT = range(5)
 
 
 class Options(C.Structure):
@@ -55,6 +55,9 @@ class Result(C.Structure):
         ("update_launches", C.c_int),
         ("direction_launches", C.c_int),
         ("fell_back", C.c_int),
+        ("inner_form", C.c_int),
+        ("inner_launches", C.c_int),
+        ("inner_ms", C.c_double),
     ]
 
     def as_dict(self):

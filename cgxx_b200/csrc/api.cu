@@ -1626,7 +1626,9 @@ static cgx_status solve_fp64(cgx_handle *h, const cgx_options &o,
     return fail(CGX_ERROR_INVALID_STATE, "Jacobi preconditioner not set");
   cudaStream_t s = h->stream;
   // The persistent mode is an inner-solve mode of the mixed paths.
-  const int loop = o.loop == CGX_LOOP_PERSISTENT ? CGX_LOOP_GRAPH : o.loop;
+  const int loop =
+      o.loop == CGX_LOOP_PERSISTENT || o.loop == CGX_LOOP_PERSISTENT_SPLIT ? CGX_LOOP_GRAPH
+                                                                           : o.loop;
 
   if (loop == CGX_LOOP_GRAPH) {
     GraphEntry *ge = nullptr;
@@ -1931,7 +1933,7 @@ static cudaError_t launch_learned_apply(cgx_handle *h, bool start) {
 // the path's start kernel(s). The grid is what the SMs hold at once, as a
 // cooperative launch requires (and no more CTAs than 256-row tiles or
 // partial-sum slots).
-static cudaError_t launch_inner_persist(cgx_handle *h, bool learned) {
+static cudaError_t launch_inner_persist(cgx_handle *h, bool learned, bool split) {
   PersistArgs a;
   a.p[0] = h->p32;
   a.p[1] = h->p32b;
@@ -1948,22 +1950,23 @@ static cudaError_t launch_inner_persist(cgx_handle *h, bool learned) {
   BandView<4> A = band_view(h);
   GBandView G{};
   if (learned) G = gband_view(h);
+  constexpr int T = kPersistThreads, F = kPersistFusedMinB;
+  constexpr int SL = kPersistSplitMinB[1], SJ = kPersistSplitMinB[0];
   void (*kern)(BandView<4>, GBandView, PersistArgs, CgState *) =
-      learned ? k_inner_persist<true> : k_inner_persist<false>;
+      split ? (learned ? k_inner_persist_split<true, T, SL> : k_inner_persist_split<false, T, SJ>)
+            : (learned ? k_inner_persist<true, T, F> : k_inner_persist<false, T, F>);
   int per_sm = 0;
-  cudaError_t e =
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, 0);
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, T, 0);
   if (e != cudaSuccess) return e;
   if (per_sm < 1) return cudaErrorCooperativeLaunchTooLarge;
-  const long long tiles = ((long long)h->N + kThreads - 1) / kThreads;
+  const long long tiles = ((long long)h->N + T - 1) / T;
   const int grid = (int)std::max<long long>(
       1, std::min<long long>({(long long)h->num_sms * per_sm, kMaxGrid, tiles}));
   e = cudaMemsetAsync(a.sync, 0, sizeof(unsigned long long), h->stream);
   if (e != cudaSuccess) return e;
   CgState *st = h->st;
   void *args[] = {&A, &G, &a, &st};
-  return cudaLaunchCooperativeKernel((const void *)kern, grid, kThreads, args, 0,
-                                     h->stream);
+  return cudaLaunchCooperativeKernel((const void *)kern, grid, T, args, 0, h->stream);
 }
 
 // The persistent inner solve needs A on the band form (offsets 0 < d1 < d2
@@ -1978,10 +1981,19 @@ static bool persist_fits(const cgx_handle *h, bool learned) {
   return true;
 }
 
-// The default loop mode runs the persistent inner solve where it measured
-// faster than the graph of per-phase kernels (kPersistMaxRows*).
-static bool persist_pays(const cgx_handle *h, bool learned) {
-  return h->N <= (learned ? kPersistMaxRows : kPersistMaxRowsJacobi);
+// Which inner solve a mixed solve runs: the graph of per-iteration kernels,
+// or a persistent launch per inner solve, fused (systems up to
+// kPersistFusedMaxRows rows) or split (larger ones). CGX_LOOP_PERSISTENT and
+// CGX_LOOP_PERSISTENT_SPLIT force their form on the band; the default
+// CGX_LOOP_GRAPH takes the persistent form that measured fastest.
+enum class InnerForm { kGraph, kFused, kSplit };
+
+static InnerForm inner_form(const cgx_handle *h, const cgx_options &o, bool learned) {
+  if (!persist_fits(h, learned)) return InnerForm::kGraph;
+  if (o.loop == CGX_LOOP_PERSISTENT) return InnerForm::kFused;
+  if (o.loop == CGX_LOOP_PERSISTENT_SPLIT) return InnerForm::kSplit;
+  if (o.loop != CGX_LOOP_GRAPH) return InnerForm::kGraph;
+  return h->N <= kPersistFusedMaxRows ? InnerForm::kFused : InnerForm::kSplit;
 }
 
 static cudaError_t launch_learned_start(cgx_handle *h) {
@@ -2038,15 +2050,18 @@ static cgx_status solve_mixed(cgx_handle *h, const cgx_options &o,
   CUDA_TRY(cudaEventRecord(h->ev[6], s));
   CGX_TRY(ensure_f32(h));
 
-  // The persistent inner solve (persist.cuh) leaves d's last update pending.
-  const bool persist = persist_fits(h, want_learned) &&
-                       (o.loop == CGX_LOOP_PERSISTENT ||
-                        (o.loop == CGX_LOOP_GRAPH && persist_pays(h, want_learned)));
+  // The persistent inner solves (persist.cuh); the fused form leaves d's
+  // last update pending.
+  const InnerForm form = inner_form(h, o, want_learned);
+  const bool persist = form != InnerForm::kGraph;
+  const bool pending = form == InnerForm::kFused;
   // PERSISTENT on a matrix without the band form runs as GRAPH.
   const bool graph_loop =
-      (o.loop == CGX_LOOP_GRAPH || o.loop == CGX_LOOP_PERSISTENT) && !persist;
+      (o.loop == CGX_LOOP_GRAPH || o.loop == CGX_LOOP_PERSISTENT ||
+       o.loop == CGX_LOOP_PERSISTENT_SPLIT) &&
+      !persist;
   auto outer_update = [&] {
-    if (persist)
+    if (pending)
       k_outer_update_pending<<<grid_stream(h, h->N), kThreads, 0, h->stream>>>(
           h->N, h->vec[CGX_VECTOR_X], h->d32, h->p32, h->p32b, h->st);
     else
@@ -2061,7 +2076,7 @@ static cgx_status solve_mixed(cgx_handle *h, const cgx_options &o,
   auto jacobi_start = [&] {
     k_inner_start<<<grid_stream(h, h->N), kThreads, 0, h->stream>>>(
         h->N, h->r64, h->r32, h->d32, h->p32, h->C32, h->st, h->partials,
-        ticket(h, kTicketInnerStart), persist ? h->z32 : nullptr);
+        ticket(h, kTicketInnerStart), pending ? h->z32 : nullptr);
     return cudaGetLastError();
   };
   GraphEntry *gj = nullptr, *gl = nullptr;
@@ -2110,11 +2125,18 @@ static cgx_status solve_mixed(cgx_handle *h, const cgx_options &o,
   double rel = 0, prev = -1;
   bool failed = false;
   int outer = 0;
-  double t_spmv = 0, t_upd = 0, t_dir = 0;
-  int launches = 0;
+  double t_spmv = 0, t_upd = 0, t_dir = 0, t_inner = 0;
+  int launches = 0, inner_launches = 0;
+  bool timed = false;  // ev[2], ev[3] bracket a persistent launch not yet read
   for (;;) {
     double r2;
     CGX_TRY(true_residual_r2(h, &r2));
+    if (timed) {
+      float ms = 0;
+      CUDA_TRY(cudaEventElapsedTime(&ms, h->ev[2], h->ev[3]));
+      t_inner += ms;
+      timed = false;
+    }
     rel = bnorm > 0 ? std::sqrt(r2) / bnorm : std::sqrt(r2);
     if (outer > 0 && (!std::isfinite(rel) || rel > 0.5 * prev)) {
       // The step failed: undo it; plain FP64 finishes below.
@@ -2145,7 +2167,11 @@ static cgx_status solve_mixed(cgx_handle *h, const cgx_options &o,
                              sizeof(unsigned long long), cudaMemcpyHostToDevice, s));
     if (persist) {
       CUDA_TRY(learned ? launch_learned_start(h) : jacobi_start());
-      CUDA_TRY(launch_inner_persist(h, learned));
+      CUDA_TRY(cudaEventRecord(h->ev[2], s));
+      CUDA_TRY(launch_inner_persist(h, learned, form == InnerForm::kSplit));
+      CUDA_TRY(cudaEventRecord(h->ev[3], s));
+      timed = true;
+      inner_launches++;
       CUDA_TRY(outer_update());
     } else if (graph_loop) {
       CUDA_TRY(cudaGraphLaunch(learned ? gl->exec : gj->exec, s));
@@ -2225,6 +2251,9 @@ static cgx_status solve_mixed(cgx_handle *h, const cgx_options &o,
   res.update_ms = t_upd;
   res.direction_ms = t_dir;
   res.spmv_launches = res.update_launches = res.direction_launches = launches;
+  res.inner_form = form == InnerForm::kFused ? 1 : form == InnerForm::kSplit ? 2 : 0;
+  res.inner_launches = inner_launches;
+  res.inner_ms = t_inner;
   return CGX_SUCCESS;
 }
 
@@ -3019,7 +3048,7 @@ cgx_status cgx_solve(cgx_handle *h, const cgx_options *opts,
   if (o.preconditioner < CGX_PRECONDITIONER_NONE ||
       o.preconditioner > CGX_PRECONDITIONER_LEARNED ||
       o.precision < CGX_PRECISION_FP64 || o.precision > CGX_PRECISION_MIXED ||
-      o.loop < CGX_LOOP_GRAPH || o.loop > CGX_LOOP_PERSISTENT)
+      o.loop < CGX_LOOP_GRAPH || o.loop > CGX_LOOP_PERSISTENT_SPLIT)
     return fail(CGX_ERROR_INVALID_ARGUMENT, "invalid option value");
   if (o.preconditioner == CGX_PRECONDITIONER_LEARNED &&
       o.precision != CGX_PRECISION_MIXED)

@@ -8,8 +8,8 @@
 // phase in the same fixed order, so all CTAs hold the same alpha, beta and
 // residual and take the same stop decision; no CTA waits for a last CTA to
 // finish a reduction, and no launch separates the phases. Vectors written
-// inside the launch are read back through L2 (__ldcg), never through the
-// read-only path, whose lines could be stale.
+// inside the launch are read with weak loads after the barrier's acquire,
+// never through the read-only path (fused.cuh).
 //
 //   learned: A  p = z + b p_old, d += a_old p_old, q = A p       | <p,q> -> a
 //            B  r = r_old - a q, y = G^T r                        | <r,r> -> test
@@ -30,21 +30,38 @@ namespace cgx {
 constexpr unsigned kSyncPolls = 1u << 24;
 enum : int { kErrGridSync = 4 };  // CgState::error: a grid barrier gave up
 
-// Largest systems the default loop mode solves with persistent inner
-// solves. The fused phases read p, z and r of neighbouring rows again, which
-// costs more as the vectors outgrow L2, and they save fewer launches on the
-// Jacobi path (two phases against five kernels for the learned one):
-// measured on the 7-point grids, learned 1.31x faster at 96^3 and 1.03x at
-// 128^3, Jacobi 1.31x faster at 96^3 and 1.08x slower at 128^3, both slower
-// at 160^3.
-#ifndef CGX_PERSIST_MAX_ROWS
-#define CGX_PERSIST_MAX_ROWS 2200000
+// Which persistent form the default loop mode takes. Measured on the 7-point
+// grids against the graph of per-iteration kernels (learned / Jacobi mixed
+// solves): fused 1.62x / 1.77x faster at 96^3; split 1.27x / 1.41x at 128^3
+// and 1.15x / 1.18x at 160^3, where the fused form's recomputed neighbour
+// values cost more than its saved barriers.
+#ifndef CGX_PERSIST_FUSED_MAX_ROWS
+#define CGX_PERSIST_FUSED_MAX_ROWS 1300000
 #endif
-#ifndef CGX_PERSIST_MAX_ROWS_JACOBI
-#define CGX_PERSIST_MAX_ROWS_JACOBI 1500000
+constexpr int kPersistFusedMaxRows = CGX_PERSIST_FUSED_MAX_ROWS;
+
+// CTA width of the persistent launches, and the CTAs per SM each kernel's
+// register budget is set for. Wide CTAs keep the grid small (148 or 296
+// CTAs), which makes the barriers and the every-CTA partial sums cheap:
+// against 256-thread CTAs (888 of them) the learned solves ran 1.2-1.3x
+// faster at every size.
+#ifndef CGX_PERSIST_THREADS
+#define CGX_PERSIST_THREADS 1024
 #endif
-constexpr int kPersistMaxRows = CGX_PERSIST_MAX_ROWS;
-constexpr int kPersistMaxRowsJacobi = CGX_PERSIST_MAX_ROWS_JACOBI;
+#ifndef CGX_PERSIST_FUSED_MINB
+#define CGX_PERSIST_FUSED_MINB 1
+#endif
+#ifndef CGX_PERSIST_SPLIT_MINB_LEARNED
+#define CGX_PERSIST_SPLIT_MINB_LEARNED 2
+#endif
+#ifndef CGX_PERSIST_SPLIT_MINB_JACOBI
+#define CGX_PERSIST_SPLIT_MINB_JACOBI 1
+#endif
+constexpr int kPersistThreads = CGX_PERSIST_THREADS;
+constexpr int kPersistFusedMinB = CGX_PERSIST_FUSED_MINB;
+constexpr int kPersistSplitMinB[2] = {CGX_PERSIST_SPLIT_MINB_JACOBI,
+                                      CGX_PERSIST_SPLIT_MINB_LEARNED};
+static_assert(kPersistThreads % 128 == 0 && kPersistThreads <= 1024, "CTA width");
 
 // Partial-sum slots: phase k of an iteration uses slot k, so a slot is
 // written again only two barriers after every CTA has read it.
@@ -76,28 +93,45 @@ __device__ __forceinline__ bool grid_sync(unsigned long long *count,
   return ok != 0;
 }
 
+// Sum over a TPB-thread CTA, valid in thread 0; sh holds TPB / 32 doubles.
+template <int TPB>
+__device__ __forceinline__ double block_sum_t(double v, double *sh) {
+  v = warp_sum(v);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) sh[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    v = lane < TPB / 32 ? sh[lane] : 0.0;
+    v = warp_sum(v);
+  }
+  return v;
+}
+
 // This CTA's partial (the block sum of v) into slot[blockIdx.x].
+template <int TPB>
 __device__ __forceinline__ void put_partial(double v, double *slot) {
-  __shared__ double sh[kWarps];
-  v = block_sum(v, sh);
+  __shared__ double sh[TPB / 32];
+  v = block_sum_t<TPB>(v, sh);
   if (threadIdx.x == 0) slot[blockIdx.x] = v;
 }
 
 // The sum of the grid's partials in a fixed order, in every thread.
+template <int TPB>
 __device__ __forceinline__ double sum_partials(const double *slot) {
-  __shared__ double sh[kWarps];
+  __shared__ double sh[TPB / 32];
   __shared__ double tot;
-  constexpr int kPer = (kMaxGrid + kThreads - 1) / kThreads;
+  constexpr int kPer = (kMaxGrid + TPB - 1) / TPB;
   double v[kPer];
 #pragma unroll
   for (int k = 0; k < kPer; k++) {
-    const int b = threadIdx.x + k * kThreads;
+    const int b = threadIdx.x + k * TPB;
     v[k] = b < (int)gridDim.x ? __ldcg(&slot[b]) : 0.0;
   }
   double s = 0.0;
 #pragma unroll
   for (int k = 0; k < kPer; k++) s += v[k];
-  s = block_sum(s, sh);
+  s = block_sum_t<TPB>(s, sh);
   if (threadIdx.x == 0) tot = s;
   __syncthreads();
   return tot;
@@ -133,8 +167,8 @@ __device__ __forceinline__ void persist_publish(CgState *st, double alpha, doubl
   if (!ok && threadIdx.x == 0) atomicOr(&st->error, kErrGridSync);
 }
 
-template <bool LEARNED>
-__global__ void __launch_bounds__(kThreads)
+template <bool LEARNED, int TPB, int MINB>
+__global__ void __launch_bounds__(TPB, MINB)
     k_inner_persist(BandView<4> A, GBandView G, PersistArgs a, CgState *st) {
   // Start state (k_inner_start / the learned start): p = z, a = b = 0.
   double rho = st->in_rho, alpha = st->in_alpha, beta = st->in_beta;
@@ -152,24 +186,24 @@ __global__ void __launch_bounds__(kThreads)
     float *p_old = par ? a.p[1] : a.p[0], *p_new = par ? a.p[0] : a.p[1];
     // A: p, d, q = A p, <p,q>.
     const DirArgs da{a.z, p_old, p_new, a.d, a.q};
-    put_partial(band_dir_rows(A, da, (float)alpha, (float)beta), slot0);
+    put_partial<TPB>(band_dir_rows<TPB>(A, da, (float)alpha, (float)beta), slot0);
     if (!(ok = grid_sync(a.sync, ++bar * nb))) break;
-    alpha = rho / sum_partials(slot0);
+    alpha = rho / sum_partials<TPB>(slot0);
     // B: r and the residual test (learned: also y = G^T r; Jacobi: z, <r,z>).
     if (LEARNED) {
       float *r_old = par ? a.r[1] : a.r[0], *r_new = par ? a.r[0] : a.r[1];
       const ResArgs ra{r_old, a.q, r_new, a.y};
-      put_partial(gband_res_rows(G, ra, (float)(-alpha)), slot1);
+      put_partial<TPB>(gband_res_rows<TPB>(G, ra, (float)(-alpha)), slot1);
     } else {
       double rr, rz;
-      inner_update_rows<true, true>(A.N, a.r[0], a.q, a.C, a.z, (float)(-alpha), rr, rz);
-      put_partial(rr, slot1);
-      put_partial(rz, slot2);
+      jacobi_res_rows<TPB>(A.N, a.r[0], a.q, a.C, a.z, (float)(-alpha), rr, rz);
+      put_partial<TPB>(rr, slot1);
+      put_partial<TPB>(rz, slot2);
     }
     if (!(ok = grid_sync(a.sync, ++bar * nb))) break;
     it++;
     total++;
-    res = sqrt(sum_partials(slot1)) / nrm0;
+    res = sqrt(sum_partials<TPB>(slot1)) / nrm0;
     const bool stop = !(res > tol) || !(fabs(alpha) <= 1.7976931348623157e308) ||
                       alpha == 0.0 || total >= maxit;
     par = 1 - par;  // this iteration's p (and r) are in the other buffers
@@ -177,15 +211,74 @@ __global__ void __launch_bounds__(kThreads)
     if (LEARNED) {
       // C: z = G y + eps C r, <r,z>.
       const GzArgs za{a.y, par ? a.r[1] : a.r[0], a.C, a.z, a.eps};
-      put_partial(gband_z_rows(G, za), slot2);
+      put_partial<TPB>(gband_z_rows<TPB>(G, za), slot2);
       if (!(ok = grid_sync(a.sync, ++bar * nb))) break;
     }
-    const double rzn = sum_partials(slot2);
+    const double rzn = sum_partials<TPB>(slot2);
     beta = rzn / rho;
     rho = rzn;
   }
   // par indexes the buffer the last phase A wrote p into.
   persist_publish(st, alpha, beta, rho, res, it, total, par, ok);
+}
+
+// The split form: the graph iteration's kernels as phases (fused.cuh), five
+// barriers per learned iteration and three per Jacobi one, no values formed
+// twice and no ping-pong buffers (p[0], r[0] only). d is complete when the
+// loop stops (the plain k_outer_update applies it).
+//
+//   learned: A  q = A p                                   | <p,q> -> a
+//            B  r -= a q, d += a p                        | <r,r> -> test
+//            C  y = G^T r                                 |
+//            D  z = G y + eps C r                         | <r,z> -> b
+//            E  p = z + b p                               |
+//   Jacobi:  A  as above                                  | <p,q> -> a
+//            B  r -= a q, d += a p                        | <r,r>, <r,Cr> -> test, b
+//            E  p = C r + b p                             |
+template <bool LEARNED, int TPB, int MINB>
+__global__ void __launch_bounds__(TPB, MINB)
+    k_inner_persist_split(BandView<4> A, GBandView G, PersistArgs a, CgState *st) {
+  double rho = st->in_rho, alpha = 0.0, beta = 0.0, res = 0.0;
+  const double nrm0 = st->in_nrm0, tol = st->in_tol;
+  int total = st->total_inner;
+  const int maxit = st->max_iter, N = A.N;
+  const unsigned long long nb = gridDim.x;
+  unsigned long long bar = 0;
+  int it = 0;
+  bool ok = true;
+  double *slot0 = a.part, *slot1 = a.part + kMaxGrid, *slot2 = a.part + 2 * kMaxGrid;
+  float *p = a.p[0], *r = a.r[0];
+  for (;;) {
+    put_partial<TPB>(band_q_rows<TPB>(A, p, a.q), slot0);
+    if (!(ok = grid_sync(a.sync, ++bar * nb))) break;
+    alpha = rho / sum_partials<TPB>(slot0);
+    {
+      double rr, rz;
+      update_rows<TPB>(N, r, a.q, a.d, p, LEARNED ? nullptr : a.C, (float)alpha, rr, rz);
+      put_partial<TPB>(rr, slot1);
+      if (!LEARNED) put_partial<TPB>(rz, slot2);
+    }
+    if (!(ok = grid_sync(a.sync, ++bar * nb))) break;
+    it++;
+    total++;
+    res = sqrt(sum_partials<TPB>(slot1)) / nrm0;
+    const bool stop = !(res > tol) || !(fabs(alpha) <= 1.7976931348623157e308) ||
+                      alpha == 0.0 || total >= maxit;
+    if (stop) break;
+    if (LEARNED) {
+      gband_t_rows<TPB>(G, r, a.y);
+      if (!(ok = grid_sync(a.sync, ++bar * nb))) break;
+      const GzArgs za{a.y, r, a.C, a.z, a.eps};
+      put_partial<TPB>(gband_z_rows<TPB>(G, za), slot2);
+      if (!(ok = grid_sync(a.sync, ++bar * nb))) break;
+    }
+    const double rzn = sum_partials<TPB>(slot2);
+    beta = rzn / rho;
+    rho = rzn;
+    direction_rows<TPB>(N, p, LEARNED ? a.z : nullptr, r, a.C, (float)beta);
+    if (!(ok = grid_sync(a.sync, ++bar * nb))) break;
+  }
+  persist_publish(st, alpha, beta, rho, res, it, total, 0, ok);
 }
 
 }  // namespace cgx

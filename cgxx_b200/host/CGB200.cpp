@@ -232,8 +232,10 @@ public:
         loop = CGX_LOOP_KERNELS;
       else if (s == "persistent")
         loop = CGX_LOOP_PERSISTENT;
+      else if (s == "split")
+        loop = CGX_LOOP_PERSISTENT_SPLIT;
       else
-        badEnv("CG_B200_LOOP", "graph, chunked, kernels, or persistent");
+        badEnv("CG_B200_LOOP", "graph, chunked, kernels, persistent, or split");
     }
     if (const char *v = std::getenv("CG_B200_DEVICE"); v && *v) {
       char *end = nullptr;
@@ -285,7 +287,8 @@ public:
       }
       static const char *loops[] = {"CUDA graph (while node)",
                                     "CUDA graph chunks", "kernel launches",
-                                    "persistent inner solves"};
+                                    "persistent inner solves",
+                                    "persistent inner solves (split)"};
       printPadded("Device loop:", loops[loop]);
     }
   }

@@ -78,15 +78,20 @@ typedef enum cgx_precision {
 
 typedef enum cgx_loop {
   CGX_LOOP_GRAPH = 0,   /* whole solve = one CUDA graph with a while node;
-                           the mixed paths on the band form switch to the
-                           persistent inner solve below where it is faster
-                           (learned: up to 2.2M rows; Jacobi: 1.5M) */
+                           the mixed paths on the band form run their inner
+                           solves as persistent launches below (PERSISTENT up
+                           to 1.3M rows, PERSISTENT_SPLIT beyond), which
+                           measured faster at every size */
   CGX_LOOP_CHUNKED = 1, /* graph of a fixed number of iterations, host polls */
   CGX_LOOP_KERNELS = 2, /* one launch per fused kernel, each timed by events */
-  CGX_LOOP_PERSISTENT = 3 /* mixed paths on the band form (the 7- and
+  CGX_LOOP_PERSISTENT = 3, /* mixed paths on the band form (the 7- and
                            5-point stencils, any size): each inner solve is
-                           one cooperative launch whose phases meet at
+                           one cooperative launch whose fused phases (three
+                           per learned iteration, two per Jacobi one) meet at
                            grid-wide barriers; other solves run as GRAPH */
+  CGX_LOOP_PERSISTENT_SPLIT = 4 /* the same launch with one phase per kernel
+                           of the GRAPH iteration (five learned, three
+                           Jacobi) and no value formed twice */
 } cgx_loop;
 
 /* Solver settings: the reference's CG_* environment switches
@@ -126,6 +131,12 @@ typedef struct cgx_result {
                             that no budget solves (e.g. singular and
                             inconsistent) ends with status CGX_SUCCESS and
                             converged = 0. */
+  int inner_form;        /* MIXED: how the inner solves ran: 0 per-iteration
+                            kernels, 1 fused persistent launches, 2 split
+                            persistent launches (cgx_loop) */
+  int inner_launches;    /* MIXED, inner_form 1 or 2: persistent launches */
+  double inner_ms;       /* MIXED, inner_form 1 or 2: their device time (CUDA
+                            events around each launch) */
 } cgx_result;
 
 /* Library ------------------------------------------------------------------ */

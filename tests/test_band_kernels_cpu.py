@@ -14,9 +14,10 @@ kernels run on a device:
     hold N rows) on 3-D and 2-D grids, grids with fewer than four offsets,
     and a band that is not a grid's;
   - the products equal A p, G y and G^T r;
-  - the persistent loop (ping-pong p and r, d one update behind and applied
-    at the end, the learned and Jacobi phase orders) gives what the unfused
-    PCG gives;
+  - the fused persistent loop (ping-pong p and r, d one update behind and
+    applied at the end, the learned and Jacobi phase orders) and the split
+    one (the graph iteration's kernels as phases) give what the unfused PCG
+    gives;
   - the partial-sum slots of the persistent phases are never rewritten
     before every CTA has read them.
 """
@@ -273,10 +274,57 @@ def test_persistent_iteration_matches_pcg(case, learned):
 
 
 @pytest.mark.parametrize("learned", [True, False])
-def test_persistent_slots_are_read_before_reuse(learned):
+@pytest.mark.parametrize("case", ["grid3d", "odd"])
+def test_split_iteration_matches_pcg(case, learned):
+    """k_inner_persist_split's phases in its order (q = A p | r -= a q,
+    d += a p | y = G^T r | z = G y + eps C r | p = z + b p, Jacobi without
+    the two factor phases and with p = C r + b p) against a plain PCG; d is
+    complete when the loop stops."""
+    A, U, Gb, d4 = _setup(case)
+    N = A.N
+    Gl, Gt = lower_csr(Gb, d4)
+    A32 = G.Crs(N, A.ptr, A.index, A.value.astype(np.float32).astype(np.float64))
+    rng = np.random.default_rng(8)
+    b = rng.standard_normal(N)
+    Cv = rng.uniform(0.5, 1.5, N).astype(np.float32)
+    eps = 0.25 if learned else 0.0
+    iters = 12
+    if learned:
+        apply = lambda r: Gl.matvec(Gt.matvec(r)) + eps * Cv * r
+    else:
+        apply = lambda r: Cv * r
+    xr = _pcg(A32, apply, b, iters)
+
+    Ub, Gbb, C = Buf(U), Buf(Gb), Buf(Cv)
+    r = b.astype(np.float32)
+    z = apply(r.astype(np.float64)).astype(np.float32)
+    p = z.copy()
+    d = np.zeros(N, np.float32)
+    rho = float(r.astype(np.float64) @ z)
+    zero = Buf(np.zeros(N))
+    for _ in range(iters):
+        _, _, q = band_dir(d4, Ub, zero, Buf(p), zero, 0.0, 1.0, N)  # q = A p
+        al = rho / float(p.astype(np.float64) @ q)
+        r = fma(-al, q, r)
+        d = fma(al, p, d)
+        if learned:
+            _, y = gband_res(d4, Gbb, Buf(r), zero, 0.0, N)  # y = G^T r
+            z = gband_z(d4, Gbb, Buf(y), Buf(r), C, eps, N)
+        else:
+            z = (Cv * r).astype(np.float32)
+        rn = float(r.astype(np.float64) @ z)
+        be, rho = rn / rho, rn
+        p = fma(be, p, z)
+    assert np.allclose(d, xr, rtol=2e-3, atol=2e-3 * np.abs(xr).max())
+
+
+@pytest.mark.parametrize("split", [False, True])
+@pytest.mark.parametrize("learned", [True, False])
+def test_persistent_slots_are_read_before_reuse(learned, split):
     """Phase k writes slot k before a barrier and every CTA reads it after
     that barrier (the Jacobi phase B writes slots 1 and 2, read after its
-    barrier). A CTA may write a slot again only once it has passed a later
+    barrier); the split form adds barriers after y = G^T r and after the
+    direction update. A CTA may write a slot again only once it has passed a later
     barrier than the one after which the slot was last read: then every CTA
     has finished reading it."""
     bar = 0
@@ -284,9 +332,12 @@ def test_persistent_slots_are_read_before_reuse(learned):
     for it in range(5):
         events = [("w", 0), ("b",), ("r", 0)]
         if learned:
-            events += [("w", 1), ("b",), ("r", 1), ("w", 2), ("b",), ("r", 2)]
+            events += [("w", 1), ("b",), ("r", 1)]
+            events += [("b",)] if split else []  # y = G^T r
+            events += [("w", 2), ("b",), ("r", 2)]
         else:
             events += [("w", 1), ("w", 2), ("b",), ("r", 1), ("r", 2)]
+        events += [("b",)] if split else []  # p = z + b p
         for e in events:
             if e[0] == "b":
                 bar += 1
@@ -296,18 +347,28 @@ def test_persistent_slots_are_read_before_reuse(learned):
                 assert e[1] not in last_read or bar > last_read[e[1]], (it, e, bar, last_read)
 
 
-def test_persistent_grid_fits_the_slots():
-    """The persistent grid (SMs x resident CTAs, at most one CTA per 256-row
-    tile) never exceeds the kMaxGrid partial-sum slots, and the grid-stride
-    row loops cover every row once."""
-    kMaxGrid, kThreads = 148 * 8, 256
-    for per_sm in (1, 4, 5, 8):
-        for N in (1, 255, 256, 257, 884736, 2200000):
-            tiles = -(-N // kThreads)
+@pytest.mark.parametrize("tpb", [256, 512, 1024])
+def test_persistent_grid_fits_the_slots(tpb):
+    """The persistent grid (SMs x resident CTAs of tpb threads, at most one
+    CTA per tpb-row tile) never exceeds the kMaxGrid partial-sum slots, and
+    the grid-stride loops cover every row once, one row per thread and four
+    per thread (with the N mod 4 tail)."""
+    kMaxGrid = 148 * 8
+    for per_sm in (1, 2048 // tpb):
+        for N in (1, 255, 256, 257, 4099, 884736):
+            tiles = -(-N // tpb)
             grid = max(1, min(148 * per_sm, kMaxGrid, tiles))
             assert grid <= kMaxGrid
             seen = np.zeros(N, np.int32)
             for blk in range(grid):
-                for start in range(blk * kThreads, N, grid * kThreads):
-                    seen[start:min(N, start + kThreads)] += 1
+                for start in range(blk * tpb, N, grid * tpb):
+                    seen[start:min(N, start + tpb)] += 1
+            assert np.all(seen == 1)
+            seen[:] = 0
+            n4 = N // 4
+            for blk in range(grid):
+                for start in range(blk * tpb, n4, grid * tpb):
+                    seen[4 * start:4 * min(n4, start + tpb)] += 1
+                for start in range(4 * n4 + blk * tpb, N, grid * tpb):
+                    seen[start:min(N, start + tpb)] += 1
             assert np.all(seen == 1)

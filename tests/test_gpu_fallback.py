@@ -30,7 +30,7 @@ def _mixed(h, A, b, precond=cg.PRECOND_JACOBI, max_iter=20000, loop=cg.LOOP_GRAP
 
 
 @pytest.mark.parametrize("loop", [cg.LOOP_GRAPH, cg.LOOP_CHUNKED, cg.LOOP_KERNELS,
-                                  cg.LOOP_PERSISTENT])
+                                  cg.LOOP_PERSISTENT, cg.LOOP_PERSISTENT_SPLIT])
 def test_fp32_overflow_falls_back_to_fp64(loop):
     """Every value of A is beyond the FP32 range (A scaled by 1e39; finite in
     FP64), so A's FP32 copy holds infinities and the inner solve cannot take a

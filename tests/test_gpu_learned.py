@@ -377,3 +377,32 @@ def test_training_gains_over_the_untrained_network():
     t, u = np.median(its["trained"]), np.median(its["untrained"])
     assert t <= 0.9 * u, its
     assert all(a < b for a, b in zip(its["trained"], its["untrained"])), its
+
+
+def test_learned_twice_as_fast_as_plain_on_heldout_fields():
+    """The learned-preconditioner mixed solve against plain FP64 Jacobi-CG on
+    8 held-out 96^3 fields of the training family (the default loop mode,
+    shipped weights): the median over fields of plain time / (learned solve
+    + set-up and inference of the factor) is at least 2, and every solve
+    reaches the FP64 1e-9 residual without falling back."""
+    from cgxx_b200 import learned as LRN
+    fam = G.Diffusion7Family(96)
+    specs = LRN.family_specs(8, 900000, 2000)
+    net = cg.Gnn(0, _shipped("diffusion7.gnn"))
+    h = cg.Handle(0)
+    h.upload_crs(fam.ptr, fam.index, fam.values(np.ones(fam.N)))
+    ratios = []
+    for k, (sigma, ell, seed) in enumerate(specs):
+        v = fam.values(G.diffusion_field(96, sigma, ell, seed))
+        A = G.Crs(fam.N, fam.ptr, fam.index, v)
+        b, _ = G.rhs_for(A, seed=k)
+        h.update_crs_values(v)
+        h.upload_jacobi(1.0 / A.diagonal())
+        LRN.solve_pair(h, fam.ptr, fam.index, v, b, True, net, 1e-4)  # warm-up
+        r = LRN.solve_pair(h, fam.ptr, fam.index, v, b, True, net, 1e-4)
+        for key in ("learned_mixed", "plain_fp64"):
+            assert r[key]["converged"] and not r[key]["fell_back"], (k, key, r[key])
+        ratios.append(r["plain_fp64"]["ms"] / (r["learned_mixed"]["ms"] + r["factor_ms"]))
+    h.close()
+    net.close()
+    assert np.median(ratios) >= 2.0, ratios

@@ -323,13 +323,12 @@ def _strided_band(N, seed):
 @pytest.mark.parametrize("case", ["diffusion7_24", "diffusion7_37x23x11", "poisson2d_65",
                                   "tridiagonal", "strided"])
 def test_band_loops_agree(handle, case):
-    """The mixed solve on the band forms in every loop mode: the grid
-    stencils (z-marching kernels, partial tiles for 37 x 23 x 11, the 2-D
-    form for the 5-point matrix; per-phase kernels in a graph, in chunks, one
-    launch at a time, and the persistent cooperative launch) and the generic
-    band kernels (tridiagonal, offsets 2 and 9, on which the persistent mode
-    runs as a graph). Every mode reaches the FP64 tolerance with inner
-    iteration counts within 2 % and the same solution."""
+    """The mixed solve on band forms (the 7-point grids, the 2-D 5-point
+    form, a tridiagonal matrix and offsets 2 and 9) in every loop mode:
+    per-iteration kernels in a graph, in chunks and one launch at a time,
+    and the fused and split persistent inner solves. Every mode reaches the
+    FP64 tolerance with inner iteration counts within 2 % and the same
+    solution."""
     A = {"diffusion7_24": lambda: G.diffusion3d(24, 7, sigma=1.0, corr_len=8.0, seed=31),
          "diffusion7_37x23x11": lambda: _grid7(37, 23, 11, seed=37),
          "poisson2d_65": lambda: G.poisson2d(65),
@@ -340,7 +339,8 @@ def test_band_loops_agree(handle, case):
     handle.upload_jacobi(1.0 / A.diagonal())
     handle.set_vector("K", b)
     out = {}
-    for loop in (cg.LOOP_GRAPH, cg.LOOP_CHUNKED, cg.LOOP_KERNELS, cg.LOOP_PERSISTENT):
+    for loop in (cg.LOOP_GRAPH, cg.LOOP_CHUNKED, cg.LOOP_KERNELS, cg.LOOP_PERSISTENT,
+                 cg.LOOP_PERSISTENT_SPLIT):
         handle.fill_vector("X", 0.0)
         r = handle.solve(max_iterations=50000, tolerance=1e-9, precision=cg.PRECISION_MIXED,
                          loop=loop)
@@ -350,7 +350,8 @@ def test_band_loops_agree(handle, case):
         out[loop] = (r, x)
     assert handle.inner_band() == _expected_band(A)
     rg, xg = out[cg.LOOP_GRAPH]
-    for loop in (cg.LOOP_CHUNKED, cg.LOOP_KERNELS, cg.LOOP_PERSISTENT):
+    for loop in (cg.LOOP_CHUNKED, cg.LOOP_KERNELS, cg.LOOP_PERSISTENT,
+                 cg.LOOP_PERSISTENT_SPLIT):
         rl, xl = out[loop]
         assert abs(rl["iterations"] - rg["iterations"]) <= 0.02 * rg["iterations"] + 2
         assert rel(xl, xg) <= 1e-6
@@ -374,8 +375,10 @@ def _grid7(nx, ny, nz, seed):
 
 
 def test_learned_loops_agree(handle):
-    """The learned path (the fused stencil iteration on the 7-point band) in
-    the three loop modes: the same iterations within 2 % and solutions."""
+    """The learned path on the 7-point band in every loop mode (the graph
+    of per-iteration kernels, chunks, single launches, and the fused and
+    split persistent inner solves): the same iterations within 2 % and
+    solutions."""
     from cgxx_b200 import learned as LRN
     A = _grid7(41, 19, 13, seed=35)
     b, _ = G.rhs_for(A, seed=36)
@@ -387,7 +390,8 @@ def test_learned_loops_agree(handle):
     handle.learned_factor(net, 1e-4)
     net.close()
     out = {}
-    for loop in (cg.LOOP_GRAPH, cg.LOOP_CHUNKED, cg.LOOP_KERNELS, cg.LOOP_PERSISTENT):
+    for loop in (cg.LOOP_GRAPH, cg.LOOP_CHUNKED, cg.LOOP_KERNELS, cg.LOOP_PERSISTENT,
+                 cg.LOOP_PERSISTENT_SPLIT):
         handle.fill_vector("X", 0.0)
         r = handle.solve(max_iterations=20000, tolerance=1e-9, precision=cg.PRECISION_MIXED,
                          preconditioner=cg.PRECOND_LEARNED, loop=loop)
@@ -396,7 +400,8 @@ def test_learned_loops_agree(handle):
         assert np.linalg.norm(b - A.matvec(x)) / np.linalg.norm(b) <= 1e-9
         out[loop] = (r["iterations"], x)
     ig, xg = out[cg.LOOP_GRAPH]
-    for loop in (cg.LOOP_CHUNKED, cg.LOOP_KERNELS, cg.LOOP_PERSISTENT):
+    for loop in (cg.LOOP_CHUNKED, cg.LOOP_KERNELS, cg.LOOP_PERSISTENT,
+                 cg.LOOP_PERSISTENT_SPLIT):
         il, xl = out[loop]
         assert abs(il - ig) <= 0.02 * ig + 2, (loop, il, ig)
         assert rel(xl, xg) <= 1e-6, loop
