@@ -19,10 +19,11 @@
 // z = G y + eps C r | p = z + b p), with the same arithmetic as those
 // kernels, so the same bits.
 //
-// The loops are those of the generic band kernels: one row per thread,
-// grid-stride over TPB-wide CTAs, the row-major band values (one 16-byte
-// load of U, one 8-byte load of the factor's row), the same products added
-// in the same order and the same masks. The band values, the factor and C do not change during a launch and
+// The loops are those of the generic band kernels: one row per thread (four
+// consecutive elements for the streaming updates), grid-stride over TPB-wide
+// CTAs, the row-major band values (one 16-byte load of U, one 8-byte load of
+// the factor's row), the same products added in the same order and the same
+// masks. The band values, the factor and C do not change during a launch and
 // take the read-only path (__ldg). The vectors are written inside the launch
 // and are read with weak loads that L1 may cache (ldv): every read of another
 // CTA's value comes after a grid barrier whose GPU-scope acquire (grid_sync)
@@ -39,8 +40,14 @@ namespace cgx {
 
 #ifndef CGX_PERSIST_LOAD_L2
 __device__ __forceinline__ float ldv(const float *p) { return __ldca(p); }
+__device__ __forceinline__ float4 ldv4(const float *v, int i) {
+  return __ldca(reinterpret_cast<const float4 *>(v) + i);
+}
 #else
 __device__ __forceinline__ float ldv(const float *p) { return __ldcg(p); }
+__device__ __forceinline__ float4 ldv4(const float *v, int i) {
+  return __ldcg(reinterpret_cast<const float4 *>(v) + i);
+}
 #endif
 
 struct DirArgs {
@@ -159,14 +166,13 @@ __device__ __forceinline__ double gband_z_rows(const GBandView &B, const GzArgs 
   return acc;
 }
 
-// One element per thread, grid-stride. (The graph's streaming kernels take
-// four consecutive elements per thread; in a persistent phase that quantum
-// leaves CTAs with 3 or 4 steps at 160^3 and 1 or 2 at 96^3, and every
-// phase lasts as long as its slowest CTA. One element per thread keeps that
-// tail near 3 %.)
-template <int TPB, typename F>
-__device__ __forceinline__ void rows1(int N, F f) {
-  for (int i = blockIdx.x * TPB + threadIdx.x; i < N; i += gridDim.x * TPB) f(i);
+// Four consecutive elements per thread (the streaming kernels' float4 loop)
+// and the tail N mod 4 one per thread.
+template <int TPB, typename F4, typename F1>
+__device__ __forceinline__ void rows4(int N, F4 f4, F1 f1) {
+  const int n4 = N >> 2;
+  for (int i = blockIdx.x * TPB + threadIdx.x; i < n4; i += gridDim.x * TPB) f4(i);
+  for (int i = 4 * n4 + blockIdx.x * TPB + threadIdx.x; i < N; i += gridDim.x * TPB) f1(i);
 }
 
 // Phase B (Jacobi): r -= a q and z = C r (k_inner_update's arithmetic);
@@ -177,14 +183,35 @@ __device__ __forceinline__ void jacobi_res_rows(int N, float *r, const float *q,
                                                 double &rr, double &rz) {
   rr = 0.0;
   rz = 0.0;
-  rows1<TPB>(N, [&](int i) {
-    const float ri = fmaf(na, ldv(q + i), ldv(r + i));
-    r[i] = ri;
-    const float zi = __ldg(C + i) * ri;
-    z[i] = zi;
+  auto dots = [&](float ri, float zi) {
     rr = fma((double)ri, (double)ri, rr);
     rz = fma((double)ri, (double)zi, rz);
-  });
+  };
+  rows4<TPB>(
+      N,
+      [&](int i) {
+        float4 rv = ldv4(r, i);
+        const float4 qv = ldv4(q, i);
+        const float4 cv = __ldg(reinterpret_cast<const float4 *>(C) + i);
+        rv.x = fmaf(na, qv.x, rv.x);
+        rv.y = fmaf(na, qv.y, rv.y);
+        rv.z = fmaf(na, qv.z, rv.z);
+        rv.w = fmaf(na, qv.w, rv.w);
+        reinterpret_cast<float4 *>(r)[i] = rv;
+        const float4 zv = make_float4(cv.x * rv.x, cv.y * rv.y, cv.z * rv.z, cv.w * rv.w);
+        reinterpret_cast<float4 *>(z)[i] = zv;
+        dots(rv.x, zv.x);
+        dots(rv.y, zv.y);
+        dots(rv.z, zv.z);
+        dots(rv.w, zv.w);
+      },
+      [&](int i) {
+        const float ri = fmaf(na, ldv(q + i), ldv(r + i));
+        r[i] = ri;
+        const float zi = __ldg(C + i) * ri;
+        z[i] = zi;
+        dots(ri, zi);
+      });
 }
 
 // ---- Split phases ----------------------------------------------------------
@@ -256,13 +283,38 @@ __device__ __forceinline__ void update_rows(int N, float *r, const float *q, flo
   const float na = -a;
   rr = 0.0;
   rz = 0.0;
-  rows1<TPB>(N, [&](int i) {
-    const float ri = fmaf(na, ldv(q + i), ldv(r + i));
-    r[i] = ri;
-    d[i] = fmaf(a, ldv(p + i), ldv(d + i));
+  auto dots = [&](float ri, float ci) {
     rr = fma((double)ri, (double)ri, rr);
-    if (C) rz = fma((double)ri, (double)(__ldg(C + i) * ri), rz);
-  });
+    if (C) rz = fma((double)ri, (double)(ci * ri), rz);
+  };
+  rows4<TPB>(
+      N,
+      [&](int i) {
+        float4 rv = ldv4(r, i), dv = ldv4(d, i);
+        const float4 qv = ldv4(q, i), pv = ldv4(p, i);
+        rv.x = fmaf(na, qv.x, rv.x);
+        rv.y = fmaf(na, qv.y, rv.y);
+        rv.z = fmaf(na, qv.z, rv.z);
+        rv.w = fmaf(na, qv.w, rv.w);
+        dv.x = fmaf(a, pv.x, dv.x);
+        dv.y = fmaf(a, pv.y, dv.y);
+        dv.z = fmaf(a, pv.z, dv.z);
+        dv.w = fmaf(a, pv.w, dv.w);
+        reinterpret_cast<float4 *>(r)[i] = rv;
+        reinterpret_cast<float4 *>(d)[i] = dv;
+        const float4 cv =
+            C ? __ldg(reinterpret_cast<const float4 *>(C) + i) : make_float4(0.f, 0.f, 0.f, 0.f);
+        dots(rv.x, cv.x);
+        dots(rv.y, cv.y);
+        dots(rv.z, cv.z);
+        dots(rv.w, cv.w);
+      },
+      [&](int i) {
+        const float ri = fmaf(na, ldv(q + i), ldv(r + i));
+        r[i] = ri;
+        d[i] = fmaf(a, ldv(p + i), ldv(d + i));
+        dots(ri, C ? __ldg(C + i) : 0.f);
+      });
 }
 
 // p = z + b p (learned, k_inner_direction_z) or p = C r + b p (Jacobi,
@@ -270,10 +322,25 @@ __device__ __forceinline__ void update_rows(int N, float *r, const float *q, flo
 template <int TPB>
 __device__ __forceinline__ void direction_rows(int N, float *p, const float *z,
                                                const float *r, const float *C, float b) {
-  rows1<TPB>(N, [&](int i) {
-    const float zi = z ? ldv(z + i) : __ldg(C + i) * ldv(r + i);
-    p[i] = fmaf(b, ldv(p + i), zi);
-  });
+  rows4<TPB>(
+      N,
+      [&](int i) {
+        const float4 pv = ldv4(p, i);
+        float4 zv;
+        if (z) {
+          zv = ldv4(z, i);
+        } else {
+          const float4 rv = ldv4(r, i), cv = __ldg(reinterpret_cast<const float4 *>(C) + i);
+          zv = make_float4(cv.x * rv.x, cv.y * rv.y, cv.z * rv.z, cv.w * rv.w);
+        }
+        reinterpret_cast<float4 *>(p)[i] =
+            make_float4(fmaf(b, pv.x, zv.x), fmaf(b, pv.y, zv.y), fmaf(b, pv.z, zv.z),
+                        fmaf(b, pv.w, zv.w));
+      },
+      [&](int i) {
+        const float zi = z ? ldv(z + i) : __ldg(C + i) * ldv(r + i);
+        p[i] = fmaf(b, ldv(p + i), zi);
+      });
 }
 
 }  // namespace cgx
