@@ -326,6 +326,8 @@ def persist_roofline(args, results, N, peak, peak_kind):
     if args.path == "plain" or not results or results[-1]["inner_form"] == 0:
         return None
     form = results[-1]["inner_form"]
+    if (form, args.path == "learned") not in PERSIST_BYTES:
+        return None  # the SELL-U form: its bytes depend on the slot counts
     full, last = PERSIST_BYTES[(form, args.path == "learned")]
     bytes_, ms, launches, its = 0, 0.0, 0, 0
     for r in results:

@@ -1933,7 +1933,9 @@ static cudaError_t launch_learned_apply(cgx_handle *h, bool start) {
 // the path's start kernel(s). The grid is what the SMs hold at once, as a
 // cooperative launch requires (and no more CTAs than 256-row tiles or
 // partial-sum slots).
-static cudaError_t launch_inner_persist(cgx_handle *h, bool learned, bool split) {
+enum class InnerForm { kGraph, kFused, kSplit, kSell };
+
+static cudaError_t launch_inner_persist(cgx_handle *h, bool learned, InnerForm form) {
   PersistArgs a;
   a.p[0] = h->p32;
   a.p[1] = h->p32b;
@@ -1947,31 +1949,65 @@ static cudaError_t launch_inner_persist(cgx_handle *h, bool learned, bool split)
   a.eps = learned ? h->L->eps : 0.f;
   a.part = h->persist_part;
   a.sync = h->persist_sync;
+  CgState *st = h->st;
+  // The grid: as many CTAs as the SMs hold, at most one per T-row tile.
+  auto grid_for = [&](const void *kern, int T, int *grid) {
+    int per_sm = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, T, 0);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorCooperativeLaunchTooLarge;
+    const long long tiles = ((long long)h->N + T - 1) / T;
+    *grid = (int)std::max<long long>(
+        1, std::min<long long>({(long long)h->num_sms * per_sm, kMaxGrid, tiles}));
+    return cudaMemsetAsync(a.sync, 0, sizeof(unsigned long long), h->stream);
+  };
+  int grid = 0;
+  cudaError_t e;
+  if (form == InnerForm::kSell) {
+    constexpr int T = kPersistSellThreads, B = kPersistSellMinB;
+    const SellUView<float> A{h->sa.meta, h->sa.off, h->sa_val, h->N};
+    SellUView<__nv_bfloat16> G{}, GT{};
+    if (learned) {
+      G = SellUView<__nv_bfloat16>{h->L->sg.meta, h->L->sg.off, h->L->sg_val, h->N};
+      GT = SellUView<__nv_bfloat16>{h->L->st.meta, h->L->st.off, h->L->st_val, h->N};
+    }
+    const void *kern = learned ? (const void *)k_inner_persist_sell<true, T, B>
+                               : (const void *)k_inner_persist_sell<false, T, B>;
+    if ((e = grid_for(kern, T, &grid)) != cudaSuccess) return e;
+    void *args[] = {(void *)&A, &G, &GT, &a, &st};
+    return cudaLaunchCooperativeKernel(kern, grid, T, args, 0, h->stream);
+  }
   BandView<4> A = band_view(h);
   GBandView G{};
   if (learned) G = gband_view(h);
   constexpr int T = kPersistThreads, F = kPersistFusedMinB;
   constexpr int SL = kPersistSplitMinB[1], SJ = kPersistSplitMinB[0];
-  void (*kern)(BandView<4>, GBandView, PersistArgs, CgState *) =
-      split ? (learned ? k_inner_persist_split<true, T, SL> : k_inner_persist_split<false, T, SJ>)
-            : (learned ? k_inner_persist<true, T, F> : k_inner_persist<false, T, F>);
-  int per_sm = 0;
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, T, 0);
-  if (e != cudaSuccess) return e;
-  if (per_sm < 1) return cudaErrorCooperativeLaunchTooLarge;
-  const long long tiles = ((long long)h->N + T - 1) / T;
-  const int grid = (int)std::max<long long>(
-      1, std::min<long long>({(long long)h->num_sms * per_sm, kMaxGrid, tiles}));
-  e = cudaMemsetAsync(a.sync, 0, sizeof(unsigned long long), h->stream);
-  if (e != cudaSuccess) return e;
-  CgState *st = h->st;
+  const bool split = form == InnerForm::kSplit;
+  const void *kern =
+      split ? (learned ? (const void *)k_inner_persist_split<true, T, SL>
+                       : (const void *)k_inner_persist_split<false, T, SJ>)
+            : (learned ? (const void *)k_inner_persist<true, T, F>
+                       : (const void *)k_inner_persist<false, T, F>);
+  if ((e = grid_for(kern, T, &grid)) != cudaSuccess) return e;
   void *args[] = {&A, &G, &a, &st};
-  return cudaLaunchCooperativeKernel((const void *)kern, grid, T, args, 0, h->stream);
+  return cudaLaunchCooperativeKernel(kern, grid, T, args, 0, h->stream);
 }
 
-// The persistent inner solve needs A on the band form (offsets 0 < d1 < d2
-// < d3, at most four), and for the learned path the factor on the band with
-// the same offsets.
+// The SELL-U form of the persistent inner solve needs A's inner product on
+// SELL-U with every slice uniform, and for the learned path G and G^T the
+// same.
+static bool sell_fits(const cgx_handle *h, bool learned) {
+  const long long slices = ((long long)h->N + 31) / 32;
+  if (!kPersistSellOn || h->band.ok || !h->sa.ok || !h->sa_val || h->sa.uniform != slices)
+    return false;
+  if (!learned) return true;
+  const Learned *L = h->L;
+  return L && !L->gb_ok && L->sell_ok && L->sg.uniform == slices && L->st.uniform == slices;
+}
+
+// The band forms need A on the band form (offsets 0 < d1 < d2 < d3, at most
+// four), and for the learned path the factor on the band with the same
+// offsets.
 static bool persist_fits(const cgx_handle *h, bool learned) {
   if (!h->band.ok || h->band.K > 4) return false;
   if (!learned) return true;
@@ -1986,9 +2022,10 @@ static bool persist_fits(const cgx_handle *h, bool learned) {
 // kPersistFusedMaxRows rows) or split (larger ones). CGX_LOOP_PERSISTENT and
 // CGX_LOOP_PERSISTENT_SPLIT force their form on the band; the default
 // CGX_LOOP_GRAPH takes the persistent form that measured fastest.
-enum class InnerForm { kGraph, kFused, kSplit };
-
 static InnerForm inner_form(const cgx_handle *h, const cgx_options &o, bool learned) {
+  if (sell_fits(h, learned) &&
+      (o.loop == CGX_LOOP_GRAPH || o.loop == CGX_LOOP_PERSISTENT_SPLIT))
+    return InnerForm::kSell;
   if (!persist_fits(h, learned)) return InnerForm::kGraph;
   if (o.loop == CGX_LOOP_PERSISTENT) return InnerForm::kFused;
   if (o.loop == CGX_LOOP_PERSISTENT_SPLIT) return InnerForm::kSplit;
@@ -2168,7 +2205,7 @@ static cgx_status solve_mixed(cgx_handle *h, const cgx_options &o,
     if (persist) {
       CUDA_TRY(learned ? launch_learned_start(h) : jacobi_start());
       CUDA_TRY(cudaEventRecord(h->ev[2], s));
-      CUDA_TRY(launch_inner_persist(h, learned, form == InnerForm::kSplit));
+      CUDA_TRY(launch_inner_persist(h, learned, form));
       CUDA_TRY(cudaEventRecord(h->ev[3], s));
       timed = true;
       inner_launches++;
@@ -2251,7 +2288,10 @@ static cgx_status solve_mixed(cgx_handle *h, const cgx_options &o,
   res.update_ms = t_upd;
   res.direction_ms = t_dir;
   res.spmv_launches = res.update_launches = res.direction_launches = launches;
-  res.inner_form = form == InnerForm::kFused ? 1 : form == InnerForm::kSplit ? 2 : 0;
+  res.inner_form = form == InnerForm::kFused ? 1
+                   : form == InnerForm::kSplit ? 2
+                   : form == InnerForm::kSell  ? 3
+                                               : 0;
   res.inner_launches = inner_launches;
   res.inner_ms = t_inner;
   return CGX_SUCCESS;

@@ -24,6 +24,7 @@
 
 #include "fused.cuh"
 #include "kernels.cuh"
+#include "sell.cuh"
 
 namespace cgx {
 
@@ -271,6 +272,110 @@ __global__ void __launch_bounds__(TPB, MINB)
       if (!(ok = grid_sync(a.sync, ++bar * nb))) break;
       const GzArgs za{a.y, r, a.C, a.z, a.eps};
       put_partial<TPB>(gband_z_rows<TPB>(G, za), slot2);
+      if (!(ok = grid_sync(a.sync, ++bar * nb))) break;
+    }
+    const double rzn = sum_partials<TPB>(slot2);
+    beta = rzn / rho;
+    rho = rzn;
+    direction_rows<TPB>(N, p, LEARNED ? a.z : nullptr, r, a.C, (float)beta);
+    if (!(ok = grid_sync(a.sync, ++bar * nb))) break;
+  }
+  persist_publish(st, alpha, beta, rho, res, it, total, 0, ok);
+}
+
+// The split form on SELL-U (sell.cuh): A, G and G^T in uniform slices (the
+// 27-point stencils and other matrices whose rows in a slice reach the same
+// neighbours), the products as sellu_rows phases with weak gathers; the
+// streaming phases and barriers are those of k_inner_persist_split.
+struct PersistQ {  // q = A p, <p,q>
+  using Acc = Acc1;
+  struct Pre {
+    float p;
+  };
+  const float *p;
+  float *q;
+  __device__ Pre prefetch(int i) const { return Pre{ldv(p + i)}; }
+  __device__ void row(int i, float s, Acc &a, const Pre &pr) const {
+    q[i] = s;
+    a.a0 = fma((double)pr.p, (double)s, a.a0);
+  }
+};
+struct PersistZ {  // z = G y + eps C r, <r,z> (OpLearnedZ's arithmetic)
+  using Acc = Acc1;
+  struct Pre {
+    float r, c;
+  };
+  const float *r, *C;
+  float *z;
+  float eps;
+  __device__ Pre prefetch(int i) const { return Pre{ldv(r + i), __ldg(C + i)}; }
+  __device__ void row(int i, float s, Acc &a, const Pre &pr) const {
+    const float zi = fmaf(eps * pr.c, pr.r, s);
+    z[i] = zi;
+    a.a0 = fma((double)pr.r, (double)zi, a.a0);
+  }
+};
+
+// Slots per chunk of the SELL-U products in the persistent form, its CTA
+// width and CTAs per SM, and whether the default loop mode takes it.
+constexpr int kPersistSellU = 8;
+#ifndef CGX_PERSIST_SELL_THREADS
+#define CGX_PERSIST_SELL_THREADS 384
+#endif
+#ifndef CGX_PERSIST_SELL_MINB
+#define CGX_PERSIST_SELL_MINB 2
+#endif
+#ifndef CGX_PERSIST_SELL
+#define CGX_PERSIST_SELL 1
+#endif
+constexpr int kPersistSellThreads = CGX_PERSIST_SELL_THREADS;
+constexpr int kPersistSellMinB = CGX_PERSIST_SELL_MINB;
+constexpr bool kPersistSellOn = CGX_PERSIST_SELL != 0;
+
+template <bool LEARNED, int TPB, int MINB>
+__global__ void __launch_bounds__(TPB, MINB)
+    k_inner_persist_sell(SellUView<float> A, SellUView<__nv_bfloat16> G,
+                         SellUView<__nv_bfloat16> GT, PersistArgs a, CgState *st) {
+  constexpr int U = kPersistSellU;
+  double rho = st->in_rho, alpha = 0.0, beta = 0.0, res = 0.0;
+  const double nrm0 = st->in_nrm0, tol = st->in_tol;
+  int total = st->total_inner;
+  const int maxit = st->max_iter, N = A.N;
+  const unsigned long long nb = gridDim.x;
+  unsigned long long bar = 0;
+  int it = 0;
+  bool ok = true;
+  double *slot0 = a.part, *slot1 = a.part + kMaxGrid, *slot2 = a.part + 2 * kMaxGrid;
+  float *p = a.p[0], *r = a.r[0];
+  for (;;) {
+    {
+      Acc1 acc;
+      sellu_rows<float, U, true, TPB>(A, p, GatherWeak{}, PersistQ{p, a.q}, acc);
+      put_partial<TPB>(acc.a0, slot0);
+    }
+    if (!(ok = grid_sync(a.sync, ++bar * nb))) break;
+    alpha = rho / sum_partials<TPB>(slot0);
+    {
+      double rr, rz;
+      update_rows<TPB>(N, r, a.q, a.d, p, LEARNED ? nullptr : a.C, (float)alpha, rr, rz);
+      put_partial<TPB>(rr, slot1);
+      if (!LEARNED) put_partial<TPB>(rz, slot2);
+    }
+    if (!(ok = grid_sync(a.sync, ++bar * nb))) break;
+    it++;
+    total++;
+    res = sqrt(sum_partials<TPB>(slot1)) / nrm0;
+    const bool stop = !(res > tol) || !(fabs(alpha) <= 1.7976931348623157e308) ||
+                      alpha == 0.0 || total >= maxit;
+    if (stop) break;
+    if (LEARNED) {
+      NoAcc none;
+      sellu_rows<__nv_bfloat16, U, true, TPB>(GT, r, GatherWeak{}, OpInnerStore{a.y}, none);
+      if (!(ok = grid_sync(a.sync, ++bar * nb))) break;
+      Acc1 acc;
+      sellu_rows<__nv_bfloat16, U, true, TPB>(G, a.y, GatherWeak{},
+                                              PersistZ{r, a.C, a.z, a.eps}, acc);
+      put_partial<TPB>(acc.a0, slot2);
       if (!(ok = grid_sync(a.sync, ++bar * nb))) break;
     }
     const double rzn = sum_partials<TPB>(slot2);

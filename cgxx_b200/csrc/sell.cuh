@@ -90,25 +90,33 @@ struct SellUView {
   int N;
 };
 
+// Gathers of x: through the read-only path (a kernel whose x is not written
+// while it runs), or with weak loads (a persistent launch, whose x another
+// CTA wrote before the last grid barrier).
+struct GatherLdg {
+  __device__ float operator()(const float *p) const { return __ldg(p); }
+};
+struct GatherWeak {
+  __device__ float operator()(const float *p) const { return __ldca(p); }
+};
+
+// The product's row loop over TPB-wide CTAs (k_sellu's body).
 // ALL_UNIFORM: the layout has no per-row slice, and its instantiation
 // leaves out the chunked per-row path (measured: carrying it costs the
 // uniform kernels 1-3 %).
-template <typename VT, int U, bool ALL_UNIFORM, typename Op>
-__global__ void __launch_bounds__(kThreads)
-    k_sellu(SellUView<VT> A, const float *__restrict__ x, Op op, CgState *st,
-            double *partials) {
-  if (op.skip(st)) return;
+template <typename VT, int U, bool ALL_UNIFORM, int TPB, typename XL, typename Op>
+__device__ __forceinline__ void sellu_rows(const SellUView<VT> &A, const float *x, XL xld,
+                                           const Op &op, typename Op::Acc &acc) {
   constexpr int SPW = 2, NG = U / 4;
-  typename Op::Acc acc;
   const int lane = threadIdx.x & 31;
   const int nslices = (A.N + 31) >> 5;
-  const int nwarps = (gridDim.x * kThreads) >> 5;
+  const int nwarps = (gridDim.x * TPB) >> 5;
   const int stride = nwarps * SPW;
   auto meta_of = [&](int s0) {
     return (lane < SPW && s0 + lane < nslices) ? __ldg(&A.meta[s0 + lane])
                                                 : make_int4(0, 0, 0, 0);
   };
-  int s0 = ((blockIdx.x * kThreads + threadIdx.x) >> 5) * SPW;
+  int s0 = ((blockIdx.x * TPB + threadIdx.x) >> 5) * SPW;
   int4 ml = meta_of(s0);
   for (; s0 < nslices; s0 += stride) {
     const int4 mn = meta_of(s0 + stride);
@@ -157,7 +165,7 @@ __global__ void __launch_bounds__(kThreads)
 #pragma unroll
           for (int u = 0; u < U; u++) {
             const int o = __shfl_sync(0xffffffffu, ol[q], (k0 + u) & 31);
-            b[q][u] = __ldg(&x[min((unsigned)(row[q] + o), nmax)]);
+            b[q][u] = xld(&x[min((unsigned)(row[q] + o), nmax)]);
           }
         }
 #pragma unroll
@@ -200,7 +208,7 @@ __global__ void __launch_bounds__(kThreads)
         for (int q = 0; q < SPW; q++)
 #pragma unroll
           for (int u = 0; u < U; u++)
-            b[q][u] = __ldg(&x[min((unsigned)(row[q] + o[q][u]), nmax)]);
+            b[q][u] = xld(&x[min((unsigned)(row[q] + o[q][u]), nmax)]);
 #pragma unroll
         for (int q = 0; q < SPW; q++)
 #pragma unroll
@@ -222,7 +230,7 @@ __global__ void __launch_bounds__(kThreads)
                                : __ldg(&A.off[ob[q] + (k << 5) + lane]);
           const float v = to_float(
               __ldg(A.val + ((((vb[q] + (k >> 2)) << 5) + lane) << 2) + (k & 3)));
-          t = fmaf(v, __ldg(&x[min(max(row[q] + o, 0), A.N - 1)]), t);
+          t = fmaf(v, xld(&x[min(max(row[q] + o, 0), A.N - 1)]), t);
         }
         sum[q] = t;
       }
@@ -232,6 +240,15 @@ __global__ void __launch_bounds__(kThreads)
       if (row[q] < A.N) op.row(row[q], sum[q], acc, pre[q]);
     ml = mn;
   }
+}
+
+template <typename VT, int U, bool ALL_UNIFORM, typename Op>
+__global__ void __launch_bounds__(kThreads)
+    k_sellu(SellUView<VT> A, const float *__restrict__ x, Op op, CgState *st,
+            double *partials) {
+  if (op.skip(st)) return;
+  typename Op::Acc acc;
+  sellu_rows<VT, U, ALL_UNIFORM, kThreads>(A, x, GatherLdg{}, op, acc);
   op.finish(acc, st, partials);
 }
 

@@ -91,7 +91,9 @@ typedef enum cgx_loop {
                            grid-wide barriers; other solves run as GRAPH */
   CGX_LOOP_PERSISTENT_SPLIT = 4 /* the same launch with one phase per kernel
                            of the GRAPH iteration (five learned, three
-                           Jacobi) and no value formed twice */
+                           Jacobi) and no value formed twice; also on SELL-U
+                           inner products whose slices are all uniform (the
+                           27-point stencils), where GRAPH takes it too */
 } cgx_loop;
 
 /* Solver settings: the reference's CG_* environment switches
@@ -133,7 +135,8 @@ typedef struct cgx_result {
                             converged = 0. */
   int inner_form;        /* MIXED: how the inner solves ran: 0 per-iteration
                             kernels, 1 fused persistent launches, 2 split
-                            persistent launches (cgx_loop) */
+                            persistent launches on the band form, 3 split
+                            persistent launches on SELL-U (cgx_loop) */
   int inner_launches;    /* MIXED, inner_form 1 or 2: persistent launches */
   double inner_ms;       /* MIXED, inner_form 1 or 2: their device time (CUDA
                             events around each launch) */

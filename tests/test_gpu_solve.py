@@ -407,6 +407,48 @@ def test_learned_loops_agree(handle):
         assert rel(xl, xg) <= 1e-6, loop
 
 
+@pytest.mark.parametrize("learned", [False, True])
+def test_sell_loops_agree(handle, learned):
+    """The mixed solves on the SELL-U inner form (27-point matrix: no band
+    form, every slice uniform) in every loop mode: the default and the split
+    persistent mode run the persistent SELL-U inner solve (inner_form 3), the
+    others the graph of per-iteration kernels; the same iterations within
+    2 % and the same solution."""
+    from cgxx_b200 import learned as LRN
+    A = G.diffusion3d(22, stencil=27, sigma=1.0, corr_len=4.0, seed=41)
+    b, _ = G.rhs_for(A, seed=42)
+    handle.upload_crs(A.ptr, A.index, A.value)
+    handle.upload_jacobi(1.0 / A.diagonal())
+    handle.set_vector("K", b)
+    pc = cg.PRECOND_JACOBI
+    if learned:
+        handle.learned_setup()
+        net = cg.Gnn(0, LRN.load_weights(LRN.DEFAULT_WEIGHTS)[0])
+        handle.learned_factor(net, 1e-4)
+        net.close()
+        pc = cg.PRECOND_LEARNED
+    out = {}
+    for loop in (cg.LOOP_GRAPH, cg.LOOP_CHUNKED, cg.LOOP_KERNELS, cg.LOOP_PERSISTENT,
+                 cg.LOOP_PERSISTENT_SPLIT):
+        handle.fill_vector("X", 0.0)
+        r = handle.solve(max_iterations=20000, tolerance=1e-9, precision=cg.PRECISION_MIXED,
+                         preconditioner=pc, loop=loop)
+        x = handle.get_vector("X")
+        assert r["converged"] == 1 and r["fell_back"] == 0, (loop, r)
+        assert np.linalg.norm(b - A.matvec(x)) / np.linalg.norm(b) <= 1e-9
+        out[loop] = (r, x)
+    assert not handle.inner_band()
+    assert out[cg.LOOP_GRAPH][0]["inner_form"] == 3
+    assert out[cg.LOOP_PERSISTENT_SPLIT][0]["inner_form"] == 3
+    assert out[cg.LOOP_PERSISTENT][0]["inner_form"] == 0  # no band: the graph
+    assert out[cg.LOOP_GRAPH][0]["inner_launches"] == out[cg.LOOP_GRAPH][0]["outer_iterations"]
+    rk, xk = out[cg.LOOP_KERNELS]
+    for loop in (cg.LOOP_GRAPH, cg.LOOP_CHUNKED, cg.LOOP_PERSISTENT, cg.LOOP_PERSISTENT_SPLIT):
+        rl, xl = out[loop]
+        assert abs(rl["iterations"] - rk["iterations"]) <= 0.02 * rk["iterations"] + 2, loop
+        assert rel(xl, xk) <= 1e-6, loop
+
+
 def test_time_spmv_measures_the_fused_product(handle):
     """cgx_time_spmv times the solver's own SpMV (FP64 and the FP32 inner
     one) back to back, and a solve afterwards is unaffected."""
