@@ -62,9 +62,11 @@ def parse_args():
     ap.add_argument("--max-iter", type=int, default=5000)
     ap.add_argument("--tol", type=float, default=1e-9)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--loop", choices=["graph", "chunked", "kernels"], default="graph",
-                    help="device loop of the timed solves (profilers need kernels: "
-                         "they cannot see inside a graph with a while node)")
+    ap.add_argument("--loop", choices=["graph", "chunked", "kernels", "persistent", "split"],
+                    default="graph",
+                    help="device loop of the timed solves (graph: the default, which runs "
+                         "the mixed paths' inner solves as persistent launches where they "
+                         "apply; profilers cannot see inside a graph with a while node)")
     ap.add_argument("--quick", action="store_true",
                     help="timed solves only (for profiler runs): no other path, "
                          "no per-kernel pass, no e2e, no CPU baseline")
@@ -363,7 +365,7 @@ def peaks():
         return 6650.0, "fallback"
 
 
-LOOPS = {"graph": 0, "chunked": 1, "kernels": 2}
+LOOPS = {"graph": 0, "chunked": 1, "kernels": 2, "persistent": 3, "split": 4}
 PATHS = ("learned", "mixed", "plain")
 
 
