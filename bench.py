@@ -56,8 +56,10 @@ def parse_args():
     ap.add_argument("--graph", type=int, default=0,
                     help="points of a random geometric graph instead of the grid")
     ap.add_argument("--path", choices=["learned", "mixed", "plain"], default="learned")
-    ap.add_argument("--weights", default=os.path.join(REPO, "cgxx_b200", "weights",
-                                                       "diffusion7.gnn"))
+    ap.add_argument("--weights", default=None,
+                    help="weight file of the learned preconditioner (default: the "
+                         "weights trained on the workload's family, diffusion7.gnn for the "
+                         "grids and graph12.gnn for --graph); 'init' for the untrained network")
     ap.add_argument("--eps", type=float, default=1e-4)
     ap.add_argument("--max-iter", type=int, default=5000)
     ap.add_argument("--tol", type=float, default=1e-9)
@@ -383,6 +385,9 @@ def load_network(args):
     present, else the untrained initialisation (reported as such)."""
     from cgxx_b200 import learned as LRN
     path = args.weights
+    if path is None:
+        path = os.path.join(REPO, "cgxx_b200", "weights",
+                            "graph12.gnn" if args.graph else "diffusion7.gnn")
     if path == "init":
         return LRN.init_params(0), {"weights": "untrained initialisation (--weights init)"}
     if path and os.path.exists(path):
@@ -594,7 +599,7 @@ def our_arm(args, world, rank, local):
             h.learned_setup()
             h.learned_factor(net, args.eps)
         r = h.solve(solve_opts(cg, args, args.path))
-        x_h[:] = h.get_vector("X")
+        h.get_vector("X", out=x_h)
         return r
 
     e2e_step()  # warm-up (graphs are rebuilt after a re-upload)

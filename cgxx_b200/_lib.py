@@ -287,8 +287,13 @@ class Handle:
         assert host.size == self.N
         check(self._lib.cgx_set_vector(self._h, VECTORS.get(v, v), p))
 
-    def get_vector(self, v):
-        out = np.empty(self.N, dtype=np.float64)
+    def get_vector(self, v, out=None):
+        """The vector as N doubles; `out` (a contiguous float64 array of N,
+        e.g. from pinned_empty) receives it instead of a new array."""
+        if out is None:
+            out = np.empty(self.N, dtype=np.float64)
+        elif out.dtype != np.float64 or out.size != self.N or not out.flags.c_contiguous:
+            raise ValueError("out must be a contiguous float64 array of N elements")
         check(self._lib.cgx_get_vector(self._h, VECTORS.get(v, v),
                                        out.ctypes.data_as(C.c_void_p)))
         return out
