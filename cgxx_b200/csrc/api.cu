@@ -690,9 +690,9 @@ static cudaError_t launch_inner_iteration(cgx_handle *h, cudaEvent_t *evs = null
   e = launch_inner_q(h);
   if (e != cudaSuccess) return e;
   if (evs) cudaEventRecord(evs[1], h->stream);
-  k_inner_update<false><<<g, kThreads, 0, h->stream>>>(
+  k_inner_update<<<g, kThreads, 0, h->stream>>>(
       h->N, h->r32, h->q32, h->C32, h->st, h->partials,
-      ticket(h, kTicketInnerUpdate), nullptr);
+      ticket(h, kTicketInnerUpdate));
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if (evs) cudaEventRecord(evs[2], h->stream);
   k_inner_direction<<<g, kThreads, 0, h->stream>>>(h->N, h->d32, h->p32,

@@ -41,7 +41,7 @@ struct CgState {
   double inner_tol_min;  // floor of the inner relative tolerance
   int in_iter, in_stop, in_finished;
   int total_inner;
-  int in_pslot;  // fused band iterations: ping-pong buffer of the last p
+  int in_pslot;  // fused persistent inner solve: ping-pong buffer of the last p
 };
 
 // The inner FP32 iteration cannot make progress: a step length that is zero

@@ -793,8 +793,8 @@ __global__ void __launch_bounds__(kThreads)
 // scalars, inside an FP64 refinement loop driven by the host.
 
 // Start: r32 = r64 / ||r64||, d = 0, p = C r32 (and z = p when z is given,
-// for the fused band iteration); <r,p>, <r,r>; a = b = 0, so that a fused
-// first iteration forms p = z and leaves d at 0.
+// for the fused persistent inner solve); <r,p>, <r,r>; a = b = 0, so that
+// its first iteration forms p = z and leaves d at 0.
 __global__ void __launch_bounds__(kThreads)
     k_inner_start(int N, const double *__restrict__ r64, float *__restrict__ r,
                   float *__restrict__ d, float *__restrict__ p,
@@ -828,17 +828,13 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 // Inner step 2: r -= a q; partial <r,r>, <r,Cr>; finalize residual test and b.
-// STORE_Z (the fused band iteration, whose first kernel reads z of
-// neighbouring rows): also z = C r, with the rounding k_inner_direction uses.
-// The loop of k_inner_update: this thread's partial sums of <r,r>, <r,z>.
-template <bool STORE_Z, bool CG = false>
-__device__ __forceinline__ void inner_update_rows(int N, float *__restrict__ r,
-                                                  const float *__restrict__ q,
-                                                  const float *__restrict__ C,
-                                                  float *__restrict__ z, float na,
-                                                  double &rr, double &rz) {
-  rr = 0.0;
-  rz = 0.0;
+__global__ void __launch_bounds__(kThreads)
+    k_inner_update(int N, float *__restrict__ r, const float *__restrict__ q,
+                   const float *__restrict__ C, CgState *st, double *partials,
+                   unsigned *ticket) {
+  if (st->in_stop) return;
+  const float na = (float)(-st->in_alpha);
+  double rr = 0.0, rz = 0.0;
   const int n4 = N >> 2;
   float4 *r4 = reinterpret_cast<float4 *>(r);
   const float4 *q4 = reinterpret_cast<const float4 *>(q);
@@ -846,8 +842,7 @@ __device__ __forceinline__ void inner_update_rows(int N, float *__restrict__ r,
   for (int i = blockIdx.x * kThreads + threadIdx.x; i < n4;
        i += gridDim.x * kThreads) {
     float4 rv = r4[i];
-    // CG: q comes from another CTA in the same persistent launch (L2 path).
-    const float4 qv = CG ? __ldcg(&q4[i]) : __ldg(&q4[i]);
+    const float4 qv = __ldg(&q4[i]);
     const float4 cv = __ldg(&c4[i]);
     rv.x = fmaf(na, qv.x, rv.x);
     rv.y = fmaf(na, qv.y, rv.y);
@@ -855,7 +850,6 @@ __device__ __forceinline__ void inner_update_rows(int N, float *__restrict__ r,
     rv.w = fmaf(na, qv.w, rv.w);
     r4[i] = rv;
     const float4 zv = make_float4(cv.x * rv.x, cv.y * rv.y, cv.z * rv.z, cv.w * rv.w);
-    if (STORE_Z) reinterpret_cast<float4 *>(z)[i] = zv;
     rr = fma((double)rv.x, (double)rv.x, rr);
     rr = fma((double)rv.y, (double)rv.y, rr);
     rr = fma((double)rv.z, (double)rv.z, rr);
@@ -867,23 +861,12 @@ __device__ __forceinline__ void inner_update_rows(int N, float *__restrict__ r,
   }
   for (int i = 4 * n4 + blockIdx.x * kThreads + threadIdx.x; i < N;
        i += gridDim.x * kThreads) {
-    const float ri = fmaf(na, CG ? __ldcg(q + i) : q[i], r[i]);
+    const float ri = fmaf(na, q[i], r[i]);
     r[i] = ri;
     const float zi = C[i] * ri;
-    if (STORE_Z) z[i] = zi;
     rr = fma((double)ri, (double)ri, rr);
     rz = fma((double)ri, (double)zi, rz);
   }
-}
-
-template <bool STORE_Z>
-__global__ void __launch_bounds__(kThreads)
-    k_inner_update(int N, float *__restrict__ r, const float *__restrict__ q,
-                   const float *__restrict__ C, CgState *st, double *partials,
-                   unsigned *ticket, float *__restrict__ z) {
-  if (st->in_stop) return;
-  double rr, rz;
-  inner_update_rows<STORE_Z>(N, r, q, C, z, (float)(-st->in_alpha), rr, rz);
   double in[2] = {rr, rz}, out[2];
   if (grid_reduce<2>(in, partials, ticket, out) && threadIdx.x == 0) {
     st->in_iter += 1;
