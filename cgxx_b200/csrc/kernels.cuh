@@ -597,11 +597,6 @@ struct OpInnerQ {
     q[i] = s;
     a.a0 = fma((double)pr.p, (double)s, a.a0);
   }
-  // Row epilogue of a product that has p_i at hand (x = p).
-  __device__ void row_x(int i, float s, Acc &a, float pi) const {
-    q[i] = s;
-    a.a0 = fma((double)pi, (double)s, a.a0);
-  }
   __device__ void finish(Acc &a, CgState *st, double *partials) const {
     double in[1] = {a.a0}, out[1];
     if (grid_reduce<1>(in, partials, ticket, out) && threadIdx.x == 0)
