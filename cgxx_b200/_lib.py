@@ -106,6 +106,7 @@ PROTOTYPES = {
     "cgx_solve": [_P, C.POINTER(Options), C.POINTER(Result)],
     "cgx_true_residual": [_P, _PD],
     "cgx_time_spmv": [_P, _I, _I, _PD],
+    "cgx_check_wait_timeout": [_P, _I, C.POINTER(C.c_int)],
     "cgx_inner_layout": [_P, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),
                          C.POINTER(C.c_longlong)],
     "cgx_inner_band": [_P, _PI, _PI],
@@ -349,6 +350,14 @@ class Handle:
         us = C.c_double()
         check(self._lib.cgx_time_spmv(self._h, int(precision), int(reps), C.byref(us)))
         return us.value
+
+    def check_wait_timeout(self, which):
+        """Runs a wait that cannot complete (0: the persistent solves' grid
+        barrier, 1: the staged products' mbarrier) until it gives up; returns
+        (status, error bits). The status is 6 (DEVICE) by design."""
+        bits = C.c_int(0)
+        st = self._lib.cgx_check_wait_timeout(self._h, int(which), C.byref(bits))
+        return st, bits.value
 
     def inner_layout(self):
         """(value_slots, uniform_slices, slices) of A's FP32 copy for the

@@ -3129,6 +3129,29 @@ cgx_status cgx_inner_matvec(cgx_handle *h, const float *x, float *y) {
   return CGX_SUCCESS;
 }
 
+cgx_status cgx_check_wait_timeout(cgx_handle *h, int which, int *error_bits) {
+  if (!h) return fail(CGX_ERROR_INVALID_ARGUMENT, "handle is NULL");
+  if ((which != 0 && which != 1) || !error_bits)
+    return fail(CGX_ERROR_INVALID_ARGUMENT, "which must be 0 or 1, error_bits not NULL");
+  CGX_TRY(need_matrix(h));
+  DeviceGuard guard(h->device);
+  CGX_TRY(ensure_rows(h));
+  CGX_TRY(ensure_f32(h));
+  reset_host_state(h, 1, 0.0, false, 0);
+  CGX_TRY(push_state(h));
+  CUDA_TRY(cudaMemsetAsync(h->persist_sync, 0, sizeof(unsigned long long), h->stream));
+  // Two CTAs, 4096 polls each: a few milliseconds before they give up.
+  k_wait_timeout<<<2, 128, 0, h->stream>>>(h->persist_sync, which, 4096u, h->st);
+  CUDA_TRY(cudaGetLastError());
+  CGX_TRY(pull_state(h));
+  *error_bits = h->host_st->error;
+  const cgx_status s = device_errors(h);
+  // The handle stays usable: the next solve starts from a clean state.
+  reset_host_state(h, 1, 0.0, false, 0);
+  CGX_TRY(push_state(h));
+  return s;
+}
+
 cgx_status cgx_time_spmv(cgx_handle *h, cgx_precision precision, int reps,
                          double *us_per_launch) {
   CGX_TRY(need_matrix(h));

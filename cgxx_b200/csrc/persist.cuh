@@ -82,17 +82,38 @@ __device__ __forceinline__ unsigned long long ld_acquire_u64(
 // the barrier are visible after it without further fences (measured 2-6 %
 // faster per solve than a full fence on each side of a relaxed add).
 __device__ __forceinline__ bool grid_sync(unsigned long long *count,
-                                          unsigned long long target) {
+                                          unsigned long long target,
+                                          unsigned polls = kSyncPolls) {
   __shared__ int ok;
   __syncthreads();
   if (threadIdx.x == 0) {
     asm volatile("red.release.gpu.global.add.u64 [%0], 1;" : : "l"(count) : "memory");
     unsigned i = 0;
-    while (ld_acquire_u64(count) < target && ++i < kSyncPolls) __nanosleep(32);
-    ok = i < kSyncPolls;
+    while (ld_acquire_u64(count) < target && ++i < polls) __nanosleep(32);
+    ok = i < polls;
   }
   __syncthreads();
   return ok != 0;
+}
+
+// Diagnostics of the bounded waits: waits that nothing can complete, with a
+// short limit, so that the give-up path runs and sets its error bit.
+//  - a grid barrier whose target the CTAs' arrivals never reach;
+//  - an mbarrier (one expected arrival) that nobody arrives on.
+__global__ void k_wait_timeout(unsigned long long *count, int which, unsigned polls,
+                               CgState *st) {
+  if (which == 0) {
+    if (!grid_sync(count, ~0ull, polls) && threadIdx.x == 0) atomicOr(&st->error, kErrGridSync);
+    return;
+  }
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  if (!mbar_wait_bounded(&bar, 0u, polls) && threadIdx.x == 0)
+    atomicOr(&st->error, kErrBarrierTimeout);
 }
 
 // Sum over a TPB-thread CTA, valid in thread 0; sh holds TPB / 32 doubles.

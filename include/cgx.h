@@ -311,6 +311,16 @@ cgx_status cgx_true_residual(cgx_handle *h, double *rel);
 cgx_status cgx_time_spmv(cgx_handle *h, cgx_precision precision, int reps,
                          double *us_per_launch);
 
+/* Diagnostics of failure detection (no counterpart in the reference): runs
+ * a kernel whose wait can never complete, with a short limit (a few
+ * milliseconds): which = 0, the grid barrier of the persistent inner solves;
+ * which = 1, the mbarrier wait of the bulk-copy staged products. The wait
+ * gives up, the kernel sets its error bit (*error_bits receives the
+ * solver state's error bits: 4 grid barrier, 1 bulk-copy wait) and returns,
+ * and the call returns CGX_ERROR_DEVICE as a solve would; the handle stays
+ * usable. Needs a matrix (for the solver scratch). */
+cgx_status cgx_check_wait_timeout(cgx_handle *h, int which, int *error_bits);
+
 /* Symmetric band form of A's FP32 copy (no counterpart in the reference):
  * when A is symmetric and all its column offsets col - row form one
  * symmetric set with at most 4 non-negative members (the 7-point

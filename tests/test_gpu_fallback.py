@@ -139,3 +139,27 @@ def test_indefinite_matrix_ends_with_a_consistent_status():
     else:
         assert r["fell_back"] == 1 or r["iterations"] >= budget, r
     assert r["iterations"] <= 2 * budget + 2
+
+
+@pytest.mark.parametrize("which,bit", [(0, 4), (1, 1)])
+def test_bounded_wait_gives_up_and_the_handle_stays_usable(which, bit):
+    """A wait that nothing can complete (0: the grid barrier of the
+    persistent inner solves, whose target the arrivals never reach; 1: an
+    mbarrier of the staged products that nobody arrives on) gives up after
+    its limit: the kernel sets its error bit and returns, the call reports
+    CGX_ERROR_DEVICE, and the same handle then solves correctly in every
+    form that uses those waits."""
+    A = G.diffusion3d(16, 7, sigma=1.0, corr_len=4.0, seed=31)
+    b, _ = G.rhs_for(A, seed=32)
+    with cg.Handle(0) as h:
+        h.upload_crs(A.ptr, A.index, A.value)
+        h.upload_jacobi(1.0 / A.diagonal())
+        h.set_vector("K", b)
+        status, bits = h.check_wait_timeout(which)
+        assert status == 6 and bits & bit, (status, bits)
+        for prec in (cg.PRECISION_FP64, cg.PRECISION_MIXED):
+            h.fill_vector("X", 0.0)
+            r = h.solve(max_iterations=5000, tolerance=1e-9, precision=prec)
+            x = h.get_vector("X")
+            assert r["converged"] == 1, r
+            assert np.linalg.norm(b - A.matvec(x)) / np.linalg.norm(b) <= 1e-9
