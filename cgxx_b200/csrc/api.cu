@@ -1982,10 +1982,14 @@ static cudaError_t launch_inner_persist(cgx_handle *h, bool learned, InnerForm f
   if (learned) G = gband_view(h);
   constexpr int T = kPersistThreads, F = kPersistFusedMinB;
   constexpr int SL = kPersistSplitMinB[1], SJ = kPersistSplitMinB[0];
+  constexpr int PF = kPersistPrefetchRows;
   const bool split = form == InnerForm::kSplit;
+  const bool pf = h->N >= kPersistPrefetchMinRows;
   const void *kern =
-      split ? (learned ? (const void *)k_inner_persist_split<true, T, SL>
-                       : (const void *)k_inner_persist_split<false, T, SJ>)
+      split ? (learned ? (pf ? (const void *)k_inner_persist_split<true, T, SL, PF>
+                             : (const void *)k_inner_persist_split<true, T, SL, 0>)
+                       : (pf ? (const void *)k_inner_persist_split<false, T, SJ, PF>
+                             : (const void *)k_inner_persist_split<false, T, SJ, 0>))
             : (learned ? (const void *)k_inner_persist<true, T, F>
                        : (const void *)k_inner_persist<false, T, F>);
   if ((e = grid_for(kern, T, &grid)) != cudaSuccess) return e;

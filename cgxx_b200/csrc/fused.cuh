@@ -50,6 +50,21 @@ __device__ __forceinline__ float4 ldv4(const float *v, int i) {
 }
 #endif
 
+// L2 prefetch of the read-only row values a thread reads PF grid-stride
+// steps later (PF = 0: none): one lane per 128-byte line issues it. It keeps
+// more of the band stream in flight than the warps' own loads (whose
+// registers cap them at one row per thread), which bounds the products
+// once the band no longer stays in L2 between iterations.
+template <int BYTES_PER_ROW, int PF>
+__device__ __forceinline__ void prefetch_row(const void *base, int i, int stride, int N) {
+  constexpr int kRowsPerLine = 128 / BYTES_PER_ROW;
+  const long long j = (long long)i + (long long)PF * stride;
+  if (PF > 0 && (threadIdx.x & (kRowsPerLine - 1)) == 0 && j < N)
+    asm volatile("prefetch.global.L2 [%0];"
+                 :
+                 : "l"((const char *)base + j * BYTES_PER_ROW));
+}
+
 struct DirArgs {
   const float *z;     // preconditioned residual
   const float *pold;  // search direction of the last iteration
@@ -67,7 +82,9 @@ __device__ __forceinline__ double band_dir_rows(const BandView<4> &B, const DirA
   const float4 *__restrict__ U4 = reinterpret_cast<const float4 *>(B.U);
   const float *z = a.z, *po = a.pold;
   double acc = 0.0;
-  for (int i = blockIdx.x * TPB + threadIdx.x; i < N; i += gridDim.x * TPB) {
+  const int stride = gridDim.x * TPB;
+  for (int i = blockIdx.x * TPB + threadIdx.x; i < N; i += stride) {
+    prefetch_row<16, 0>(B.U, i, stride, N);
     const float4 u = __ldg(U4 + i);
     const float po0 = ldv(po + i);
     const float p0 = fmaf(be, po0, ldv(z + i));
@@ -111,7 +128,9 @@ __device__ __forceinline__ double gband_res_rows(const GBandView &B, const ResAr
   const unsigned short *gv = reinterpret_cast<const unsigned short *>(B.val);
   const float *ro = a.rold, *qv = a.q;
   double rr = 0.0;
-  for (int i = blockIdx.x * TPB + threadIdx.x; i < N; i += gridDim.x * TPB) {
+  const int stride = gridDim.x * TPB;
+  for (int i = blockIdx.x * TPB + threadIdx.x; i < N; i += stride) {
+    prefetch_row<8, 0>(B.val, i, stride, N);
     const float r0 = fmaf(na, ldv(qv + i), ldv(ro + i));
     float v[4], xv[4];
     v[0] = bf16_bits_to_float(__ldg(&gv[(size_t)i * 4]));
@@ -141,12 +160,14 @@ struct GzArgs {
 };
 
 // Phase C (learned): z = G y + eps C r; this thread's partial sum of <r,z>.
-template <int TPB>
+template <int TPB, int PF = 0>
 __device__ __forceinline__ double gband_z_rows(const GBandView &B, const GzArgs &a) {
   const int N = B.N;
   const float *y = a.y;
   double acc = 0.0;
-  for (int i = blockIdx.x * TPB + threadIdx.x; i < N; i += gridDim.x * TPB) {
+  const int stride = gridDim.x * TPB;
+  for (int i = blockIdx.x * TPB + threadIdx.x; i < N; i += stride) {
+    prefetch_row<8, PF>(B.val, i, stride, N);
     const uint2 raw = __ldg(reinterpret_cast<const uint2 *>(B.val) + i);
     float v[4], xv[4];
     v[0] = __uint_as_float(raw.x << 16);
@@ -217,14 +238,16 @@ __device__ __forceinline__ void jacobi_res_rows(int N, float *r, const float *q,
 // ---- Split phases ----------------------------------------------------------
 
 // q = A p; this thread's partial of <p,q> (k_band with OpInnerQ).
-template <int TPB>
+template <int TPB, int PF = 0>
 __device__ __forceinline__ double band_q_rows(const BandView<4> &B, const float *p,
                                               float *q) {
   const int N = B.N;
   const unsigned nmax = (unsigned)(N - 1);
   const float4 *__restrict__ U4 = reinterpret_cast<const float4 *>(B.U);
   double acc = 0.0;
-  for (int i = blockIdx.x * TPB + threadIdx.x; i < N; i += gridDim.x * TPB) {
+  const int stride = gridDim.x * TPB;
+  for (int i = blockIdx.x * TPB + threadIdx.x; i < N; i += stride) {
+    prefetch_row<16, PF>(B.U, i, stride, N);
     const float4 u = __ldg(U4 + i);
     float xu[4], lv[4], xl[4];
 #pragma unroll
@@ -249,11 +272,13 @@ __device__ __forceinline__ double band_q_rows(const BandView<4> &B, const float 
 }
 
 // y = G^T r (k_gband<true> with OpInnerStore).
-template <int TPB>
+template <int TPB, int PF = 0>
 __device__ __forceinline__ void gband_t_rows(const GBandView &B, const float *r, float *y) {
   const int N = B.N;
   const unsigned short *gv = reinterpret_cast<const unsigned short *>(B.val);
-  for (int i = blockIdx.x * TPB + threadIdx.x; i < N; i += gridDim.x * TPB) {
+  const int stride = gridDim.x * TPB;
+  for (int i = blockIdx.x * TPB + threadIdx.x; i < N; i += stride) {
+    prefetch_row<8, PF>(B.val, i, stride, N);
     float v[4], xv[4];
     v[0] = bf16_bits_to_float(__ldg(&gv[(size_t)i * 4]));
     xv[0] = ldv(r + i);

@@ -41,6 +41,16 @@ enum : int { kErrGridSync = 4 };  // CgState::error: a grid barrier gave up
 #endif
 constexpr int kPersistFusedMaxRows = CGX_PERSIST_FUSED_MAX_ROWS;
 
+// Systems from this size on take the split kernel with an L2 prefetch of
+// the band values two grid-stride rows ahead (measured at 160^3: learned /
+// Jacobi solves 2 % / 6 % faster; at 128^3, where the band stays in L2,
+// 1-3 % slower).
+#ifndef CGX_PERSIST_PREFETCH_MIN_ROWS
+#define CGX_PERSIST_PREFETCH_MIN_ROWS 3000000
+#endif
+constexpr int kPersistPrefetchMinRows = CGX_PERSIST_PREFETCH_MIN_ROWS;
+constexpr int kPersistPrefetchRows = 2;
+
 // CTA width of the persistent launches, and the CTAs per SM each kernel's
 // register budget is set for. Wide CTAs keep the grid small (148 or 296
 // CTAs), which makes the barriers and the every-CTA partial sums cheap:
@@ -258,7 +268,7 @@ __global__ void __launch_bounds__(TPB, MINB)
 //   Jacobi:  A  as above                                  | <p,q> -> a
 //            B  r -= a q, d += a p                        | <r,r>, <r,Cr> -> test, b
 //            E  p = C r + b p                             |
-template <bool LEARNED, int TPB, int MINB>
+template <bool LEARNED, int TPB, int MINB, int PF>
 __global__ void __launch_bounds__(TPB, MINB)
     k_inner_persist_split(BandView<4> A, GBandView G, PersistArgs a, CgState *st) {
   double rho = st->in_rho, alpha = 0.0, beta = 0.0, res = 0.0;
@@ -272,7 +282,7 @@ __global__ void __launch_bounds__(TPB, MINB)
   double *slot0 = a.part, *slot1 = a.part + kMaxGrid, *slot2 = a.part + 2 * kMaxGrid;
   float *p = a.p[0], *r = a.r[0];
   for (;;) {
-    put_partial<TPB>(band_q_rows<TPB>(A, p, a.q), slot0);
+    put_partial<TPB>(band_q_rows<TPB, PF>(A, p, a.q), slot0);
     if (!(ok = grid_sync(a.sync, ++bar * nb))) break;
     alpha = rho / sum_partials<TPB>(slot0);
     {
@@ -289,10 +299,10 @@ __global__ void __launch_bounds__(TPB, MINB)
                       alpha == 0.0 || total >= maxit;
     if (stop) break;
     if (LEARNED) {
-      gband_t_rows<TPB>(G, r, a.y);
+      gband_t_rows<TPB, PF>(G, r, a.y);
       if (!(ok = grid_sync(a.sync, ++bar * nb))) break;
       const GzArgs za{a.y, r, a.C, a.z, a.eps};
-      put_partial<TPB>(gband_z_rows<TPB>(G, za), slot2);
+      put_partial<TPB>(gband_z_rows<TPB, PF>(G, za), slot2);
       if (!(ok = grid_sync(a.sync, ++bar * nb))) break;
     }
     const double rzn = sum_partials<TPB>(slot2);

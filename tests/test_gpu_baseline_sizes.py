@@ -115,3 +115,45 @@ def test_band_inner_product_at_benchmark_size():
     absA = G.Crs(A.N, A.ptr, A.index, np.abs(A.value))
     bound = 4e-6 * absA.matvec(np.abs(xd)) + 1e-30
     assert np.all(np.abs(y.astype(np.float64) - ref) <= bound)
+
+
+@pytest.mark.parametrize("learned", [False, True])
+def test_mixed_paths_at_benchmark_size(learned):
+    """The mixed and learned solves on the benchmark matrix (160^3, so the
+    split persistent kernel with its L2 prefetch of the band values, and the
+    fused form and the per-iteration kernels for comparison): every loop
+    mode reaches the FP64 1e-9 true residual with inner iteration counts
+    within 2 %, and its solution is within 1e-6 of the FP64 solve's (the
+    plain path, the reference's algorithm)."""
+    from cgxx_b200 import learned as LRN
+    A, _, k = _workload("diffusion7_160")
+    with cg.Handle(0) as h:
+        h.upload_crs(A.ptr, A.index, A.value)
+        h.upload_jacobi(1.0 / A.diagonal())
+        h.set_vector("K", k)
+        h.fill_vector("X", 0.0)
+        r64 = h.solve(max_iterations=MAX_ITER, tolerance=TOL)
+        x64 = h.get_vector("X")
+        assert r64["converged"] == 1
+        pc = cg.PRECOND_JACOBI
+        if learned:
+            net = cg.Gnn(0, LRN.load_weights(LRN.DEFAULT_WEIGHTS)[0])
+            h.learned_setup()
+            h.learned_factor(net, 1e-4)
+            net.close()
+            pc = cg.PRECOND_LEARNED
+        out = {}
+        for loop in (cg.LOOP_GRAPH, cg.LOOP_PERSISTENT, cg.LOOP_KERNELS):
+            h.fill_vector("X", 0.0)
+            r = h.solve(max_iterations=20000, tolerance=TOL, precision=cg.PRECISION_MIXED,
+                        preconditioner=pc, loop=loop)
+            x = h.get_vector("X")
+            assert r["converged"] == 1 and r["fell_back"] == 0, (loop, r)
+            assert np.linalg.norm(k - A.matvec(x)) / np.linalg.norm(k) <= TOL, loop
+            assert np.linalg.norm(x - x64) / np.linalg.norm(x64) <= 1e-6, loop
+            out[loop] = r
+    assert out[cg.LOOP_GRAPH]["inner_form"] == 2
+    assert out[cg.LOOP_PERSISTENT]["inner_form"] == 1
+    ik = out[cg.LOOP_KERNELS]["iterations"]
+    for loop in (cg.LOOP_GRAPH, cg.LOOP_PERSISTENT):
+        assert abs(out[loop]["iterations"] - ik) <= 0.02 * ik + 2, (loop, out[loop], ik)
