@@ -2002,7 +2002,7 @@ static cudaError_t launch_inner_persist(cgx_handle *h, bool learned, InnerForm f
 // same.
 static bool sell_fits(const cgx_handle *h, bool learned) {
   const long long slices = ((long long)h->N + 31) / 32;
-  if (!kPersistSellOn || h->band.ok || !h->sa.ok || !h->sa_val || h->sa.uniform != slices)
+  if (h->band.ok || !h->sa.ok || !h->sa_val || h->sa.uniform != slices)
     return false;
   if (!learned) return true;
   const Learned *L = h->L;

@@ -348,7 +348,7 @@ struct PersistZ {  // z = G y + eps C r, <r,z> (OpLearnedZ's arithmetic)
 };
 
 // Slots per chunk of the SELL-U products in the persistent form, its CTA
-// width and CTAs per SM, and whether the default loop mode takes it.
+// width and CTAs per SM.
 // Measured on the 27-point grids (Jacobi / learned mixed solves against the
 // graph of per-iteration kernels): 1.30x / 1.29x faster at 96^3, 1.17x /
 // 1.20x at 128^3, with 512-thread CTAs two per SM (64 registers, a few
@@ -360,12 +360,8 @@ constexpr int kPersistSellU = 8;
 #ifndef CGX_PERSIST_SELL_MINB
 #define CGX_PERSIST_SELL_MINB 2
 #endif
-#ifndef CGX_PERSIST_SELL
-#define CGX_PERSIST_SELL 1
-#endif
 constexpr int kPersistSellThreads = CGX_PERSIST_SELL_THREADS;
 constexpr int kPersistSellMinB = CGX_PERSIST_SELL_MINB;
-constexpr bool kPersistSellOn = CGX_PERSIST_SELL != 0;
 
 template <bool LEARNED, int TPB, int MINB>
 __global__ void __launch_bounds__(TPB, MINB)
