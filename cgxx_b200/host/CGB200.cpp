@@ -280,6 +280,12 @@ public:
       if (precision == CGX_PRECISION_MIXED) {
         printPadded("Refinement steps:", std::to_string(last.outer_iterations));
         printPadded("Fell back to FP64:", last.fell_back ? "yes" : "no");
+        static const char *forms[] = {"per-iteration kernels",
+                                      "persistent, fused (band)",
+                                      "persistent, split (band)",
+                                      "persistent, split (SELL-U)"};
+        const int f = last.inner_form >= 0 && last.inner_form <= 3 ? last.inner_form : 0;
+        printPadded("Inner solves:", forms[f]);
       }
       if (gnn) {
         printPadded("Learned factor:", learnedFile);

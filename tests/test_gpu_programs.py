@@ -81,6 +81,7 @@ def test_cg_b200_mixed_precision():
     s = O.parse_summary(out)
     assert s["residual"][0] <= 1e-9 and s["correct"] == 1
     assert "Refinement steps:" in out
+    assert "Inner solves:" in out
 
 
 @pytest.mark.skipif(ADAPTER is None, reason="oracle/_ref/cg_b200_kernels not built")
