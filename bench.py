@@ -620,15 +620,18 @@ def our_arm(args, world, rank, local):
     # Persistent inner solves: one cooperative launch per refinement step
     # after its start.
     persist = args.path != "plain" and res["inner_form"] != 0
+    # Per solve: the fill of x, the dot of ||b||, a true-residual product per
+    # refinement check (outer + 1), and per refinement step its start, the
+    # inner solve and the update of x; the learned path adds its set-up
+    # (2 kernels), inference (6) and the start's apply (2 per step).
     if args.path == "plain":
         per_solve = 2 + 4 * iters                   # fill, set-up, 3 fused + guard
     elif args.path == "mixed":
-        # dot, true residuals, start, update; per iteration 3 kernels + guard
-        per_solve = 2 + 3 * outer + 1 + (2 * outer if persist else 4 * iters)
+        inner = outer if persist else 4 * iters     # one launch, or 3 kernels + guard
+        per_solve = 2 + (outer + 1) + 2 * outer + inner
     else:
-        # + set-up and network; per iteration 5 kernels + guard + the
-        # start's apply (persistent: start, apply, one solve, update)
-        per_solve = 2 + 19 + 3 * outer + 1 + 3 * outer + (2 * outer if persist else 7 * iters)
+        inner = outer if persist else 6 * iters     # one launch, or 5 kernels + guard
+        per_solve = 2 + 8 + (outer + 1) + 4 * outer + inner
     launches = args.steps * per_solve
 
     cpu = None
