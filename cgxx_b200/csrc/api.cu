@@ -608,7 +608,7 @@ static cudaError_t launch_pcg_setup(cgx_handle *h, bool jacobi) {
 
 // q = A p in FP32 with <p,q> (inner solves), compact indices when they fit.
 // k_sellu over one wave of CTAs (as many as fit on the SMs at once), fewer
-// when the slice pairs run out; chunks of 4 slots when no slice is wider,
+// when the warp steps run out; chunks of 4 slots when no slice is wider,
 // and the uniform-only kernel when every slice is uniform.
 template <typename VT, int U, bool ALL_UNIFORM, typename Op>
 static cudaError_t launch_sellu_u(cgx_handle *h, SellUView<VT> A, const float *x,
@@ -618,9 +618,11 @@ static cudaError_t launch_sellu_u(cgx_handle *h, SellUView<VT> A, const float *x
   cudaError_t e =
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, 0);
   if (e != cudaSuccess) return e;
-  const int pairs = ((h->N + 31) / 32 + 1) / 2;
+  // Warp steps: slice pairs on a uniform layout, single slices otherwise.
+  const int slices = (h->N + 31) / 32;
+  const int steps = ALL_UNIFORM ? (slices + 1) / 2 : slices;
   const int grid = std::max(1, std::min(h->num_sms * std::max(1, per_sm),
-                                        (pairs + kWarps - 1) / kWarps));
+                                        (steps + kWarps - 1) / kWarps));
   kern<<<grid, kThreads, 0, h->stream>>>(A, x, op, h->st, h->partials);
   return cudaGetLastError();
 }

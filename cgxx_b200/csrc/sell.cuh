@@ -72,9 +72,13 @@ __device__ __forceinline__ float4 load_group(const __nv_bfloat16 *p) {
 }
 
 // SELL-U SpMV with the row epilogue of Op (the same Ops as k_crs, with the
-// row's own operands prefetched). Warps take SPW = 2 slices per step
-// (grid-stride over slice pairs, so the warps of the grid sweep the value
-// array together) and load the next step's slice meta one step ahead. A
+// row's own operands prefetched). Warps take SPW slices per step
+// (grid-stride, so the warps of the grid sweep the value array together)
+// and load the next step's slice meta one step ahead: two slices on a
+// uniform layout, one on a layout with per-row slices, whose steps run to
+// the wider slice's width (measured on the 2M-point geometric graph's
+// factor: the learned solve 43.4 against 46.2 ms with one slice per warp;
+// chunks of 16 slots instead of 8, 47.6 ms). A
 // uniform slice is processed in chunks of U slots whose loads are all
 // unconditional: groups and gathers past the slice's width re-read its last
 // ones (L1 hits) and are masked out, so every value load and gather of a
@@ -107,7 +111,7 @@ struct GatherWeak {
 template <typename VT, int U, bool ALL_UNIFORM, int TPB, typename XL, typename Op>
 __device__ __forceinline__ void sellu_rows(const SellUView<VT> &A, const float *x, XL xld,
                                            const Op &op, typename Op::Acc &acc) {
-  constexpr int SPW = 2, NG = U / 4;
+  constexpr int SPW = ALL_UNIFORM ? 2 : 1, NG = U / 4;
   const int lane = threadIdx.x & 31;
   const int nslices = (A.N + 31) >> 5;
   const int nwarps = (gridDim.x * TPB) >> 5;

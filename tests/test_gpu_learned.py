@@ -75,7 +75,9 @@ def test_factor_matches_oracle(name, make):
 @pytest.mark.parametrize("name,make", MATRICES + [
     ("diffusion7_13", lambda: G.diffusion3d(13, 7, sigma=1.0, corr_len=4.0, seed=5)),
     ("poisson2d_37", lambda: G.poisson2d(37)),
-], ids=[m[0] for m in MATRICES] + ["diffusion7_13", "poisson2d_37"])
+    # per-row SELL-U slices
+    ("graph_4500", lambda: G.geometric_graph(4500, seed=5)),
+], ids=[m[0] for m in MATRICES] + ["diffusion7_13", "poisson2d_37", "graph_4500"])
 def test_apply_matches_factor(name, make):
     """z = G (G^T r) + eps C r from the device (BF16 factor values, the band
     copy of G for the 7- and 5-point stencils, SELL-U or FP32 CRS otherwise)
