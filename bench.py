@@ -377,7 +377,7 @@ def solve_opts(cg, args, path, loop=None):
     return cg.default_options(
         max_iterations=args.max_iter, tolerance=args.tol, preconditioner=pc,
         precision=prec, loop=LOOPS[args.loop] if loop is None else loop,
-        inner_tolerance=1e-5, max_outer=30)
+        inner_tolerance=3e-6, max_outer=30)
 
 
 def load_network(args):

@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <climits>
 #include <cmath>
 #include <cstdio>
@@ -211,6 +212,9 @@ struct cgx_handle {
   unsigned long long *persist_sync = nullptr;
   double *r64 = nullptr;
   bool f32_valid = false;
+  // What the captured inner-solve graphs took from the FP32 copy (its
+  // buffers, index form and band / SELL-U layout) when they were built.
+  std::array<uintptr_t, 10> f32_key{};
   // SELL-U copy of A's FP32 values for the inner SpMV (built with the FP32
   // mirror; sa.ok when the layout's indices fit in int).
   SellU sa;
@@ -874,7 +878,7 @@ cgx_status cgx_default_options(cgx_options *o) {
   o->preconditioner = CGX_PRECONDITIONER_JACOBI;
   o->precision = CGX_PRECISION_FP64;
   o->loop = CGX_LOOP_GRAPH;
-  o->inner_tolerance = 1e-5;
+  o->inner_tolerance = 3e-6;
   o->max_outer = 30;
   o->compute_true_residual = 0;
   return CGX_SUCCESS;
@@ -1877,7 +1881,19 @@ static cgx_status ensure_f32(cgx_handle *h) {
                            cudaMemcpyDeviceToHost, h->stream));
   CUDA_TRY(cudaStreamSynchronize(h->stream));
   h->compact16 = *(int *)h->host_scalar == 0;
-  drop_graphs(h);  // the inner graphs depend on the index form
+  // The graphs hold pointers and layout choices, not values: a refresh that
+  // keeps them keeps the graphs. (Destroying the executable graphs on every
+  // refresh cost the first solve after it up to 40 ms of host time now and
+  // then.)
+  const std::array<uintptr_t, 10> key = {
+      (uintptr_t)h->value32, (uintptr_t)h->idx16,  (uintptr_t)h->compact16,
+      (uintptr_t)h->band.U,  (uintptr_t)h->band.K, (uintptr_t)h->band.ok,
+      (uintptr_t)h->sa.meta, (uintptr_t)h->sa_val, (uintptr_t)h->sa.ok,
+      (uintptr_t)h->C32};
+  if (key != h->f32_key) {
+    drop_graphs(h);
+    h->f32_key = key;
+  }
   h->f32_valid = true;
   return CGX_SUCCESS;
 }

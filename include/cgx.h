@@ -104,7 +104,7 @@ typedef struct cgx_options {
   int preconditioner;      /* cgx_preconditioner (default JACOBI) */
   int precision;           /* cgx_precision (default FP64) */
   int loop;                /* cgx_loop (default GRAPH) */
-  double inner_tolerance;  /* MIXED: floor of the inner relative tolerance */
+  double inner_tolerance;  /* MIXED: floor of the inner relative tolerance (3e-6) */
   int max_outer;           /* MIXED: limit on refinement steps */
   int compute_true_residual; /* FP64 ||k - A x|| / ||k|| after the solve */
 } cgx_options;

@@ -160,9 +160,10 @@ def _solve(m, N, k, Cdiag, x0, max_iter, tol, keep):
 
 
 def mixed_ir_solve(ptr, index, value, Cdiag, b, max_iter=10000, tol=1e-9,
-                   inner_tol=1e-5, max_outer=30):
-    """FP32-inner / FP64-refinement restatement (see cg_oracle.h). Returns
-    (x, total_inner, outer, true_residual)."""
+                   inner_tol=3e-6, max_outer=30):
+    """FP32-inner / FP64-refinement restatement (see cg_oracle.h), with the
+    library's default floor of the inner tolerance. Returns (x, total_inner,
+    outer, true_residual)."""
     ptr, index, value = _c(ptr, np.int32), _c(index, np.int32), _c(value, np.float64)
     Cd, b = _c(Cdiag, np.float64), _c(b, np.float64)
     N = len(ptr) - 1
