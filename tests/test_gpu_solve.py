@@ -572,3 +572,57 @@ def test_mixed_and_learned_accept_every_format():
         im2, xm2, il2, xl2, band2 = out[fmt]
         assert band2 == band and im2 == im and il2 == il, fmt
         assert rel(xm2, xm) <= 1e-10 and rel(xl2, xl) <= 1e-10, fmt
+
+
+@pytest.mark.parametrize("case", ["graph", "stencil27", "band7"])
+def test_value_refresh_keeps_graphs_and_results(case):
+    """A value refresh of the same pattern keeps the captured inner-solve
+    graphs (they hold pointers and layout choices, not values). The mixed
+    and learned solves after each refresh give exactly what a fresh handle
+    gives for those values: on the graph of per-iteration kernels (FP32 CRS
+    and per-row SELL-U), on the persistent SELL-U form and on the band, and
+    in the chunked loop's captured graph on each."""
+    from cgxx_b200 import learned as LRN
+    if case == "graph":
+        # the same points with new weights: same pattern, symmetric scaling
+        base = G.geometric_graph(6000, seed=31)
+        rng = np.random.default_rng(5)
+        rows = np.repeat(np.arange(base.N), np.diff(base.ptr))
+        f = rng.uniform(0.5, 2.0, base.N)
+        v = base.value * np.sqrt(f[rows] * f[base.index])
+        mats = [base, G.Crs(base.N, base.ptr, base.index, v)]
+    elif case == "stencil27":
+        mats = [G.diffusion3d(12, stencil=27, seed=s) for s in (33, 34)]
+    else:
+        mats = [G.diffusion3d(13, stencil=7, seed=s) for s in (35, 36)]
+    assert np.array_equal(mats[0].index, mats[1].index)
+    net = cg.Gnn(0, LRN.init_params(2))
+
+    def solves(h, A):
+        b, _ = G.rhs_for(A, seed=7)
+        h.upload_jacobi(1.0 / A.diagonal())
+        h.set_vector("K", b)
+        out = []
+        for pc in (cg.PRECOND_JACOBI, cg.PRECOND_LEARNED):
+            if pc == cg.PRECOND_LEARNED:
+                h.learned_setup()
+                h.learned_factor(net, 1e-4)
+            # the default loop, and the chunked graph (captured on every form)
+            for loop in (cg.LOOP_GRAPH, cg.LOOP_CHUNKED):
+                h.fill_vector("X", 0.0)
+                r = h.solve(max_iterations=5000, tolerance=1e-9,
+                            precision=cg.PRECISION_MIXED, preconditioner=pc, loop=loop)
+                out.append((r["iterations"], r["inner_form"], h.get_vector("X")))
+        return out
+
+    with cg.Handle(0) as h:
+        h.upload_crs(mats[0].ptr, mats[0].index, mats[0].value)
+        for k in (0, 1, 0, 1):
+            h.update_crs_values(mats[k].value)
+            got = solves(h, mats[k])
+            with cg.Handle(0) as fresh:
+                fresh.upload_crs(mats[k].ptr, mats[k].index, mats[k].value)
+                ref = solves(fresh, mats[k])
+            for (it, form, x), (it0, form0, x0) in zip(got, ref):
+                assert it == it0 and form == form0 and np.array_equal(x, x0), (case, k)
+    net.close()
