@@ -319,6 +319,10 @@ def _read_profile(name):
 #   fused Jacobi:  p, d, q 40 | r, z 20
 PERSIST_BYTES = {(2, True): (100, 48), (2, False): (68, 52),
                  (1, True): (88, 64), (1, False): (60, 60)}
+# The learned split form on grids of at least 3M rows (its L2-prefetch
+# variant) applies d += a p in the direction phase, reading p once.
+PERSIST_DEFER_MIN_ROWS = 3_000_000
+PERSIST_BYTES_DEFERRED = {(2, True): (96, 36)}
 PERSIST_KERNEL = {(2, True): "k_inner_persist_split<learned>", (2, False): "k_inner_persist_split<Jacobi>",
                   (1, True): "k_inner_persist<learned>", (1, False): "k_inner_persist<Jacobi>"}
 
@@ -332,7 +336,9 @@ def persist_roofline(args, results, N, peak, peak_kind):
     form = results[-1]["inner_form"]
     if (form, args.path == "learned") not in PERSIST_BYTES:
         return None  # the SELL-U form: its bytes depend on the slot counts
-    full, last = PERSIST_BYTES[(form, args.path == "learned")]
+    key = (form, args.path == "learned")
+    full, last = (PERSIST_BYTES_DEFERRED[key] if key in PERSIST_BYTES_DEFERRED
+                  and N >= PERSIST_DEFER_MIN_ROWS else PERSIST_BYTES[key])
     bytes_, ms, launches, its = 0, 0.0, 0, 0
     for r in results:
         if r["fell_back"] or r["inner_launches"] == 0:
@@ -343,7 +349,6 @@ def persist_roofline(args, results, N, peak, peak_kind):
         its += r["iterations"]
     if launches == 0 or ms <= 0:
         return None
-    key = (form, args.path == "learned")
     out = {"bound": "hbm", "achieved": bytes_ / (ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
            "kernel": PERSIST_KERNEL[key] + ": one inner solve per launch",
            "launch_us": 1e3 * ms / launches, "launches": launches,

@@ -2109,11 +2109,16 @@ static cgx_status solve_mixed(cgx_handle *h, const cgx_options &o,
   CUDA_TRY(cudaEventRecord(h->ev[6], s));
   CGX_TRY(ensure_f32(h));
 
-  // The persistent inner solves (persist.cuh); the fused form leaves d's
-  // last update pending.
+  // The persistent inner solves (persist.cuh): the fused form, and the split
+  // one where persist_defers_d, leave d's last update pending; the fused
+  // form's start also stores z.
   const InnerForm form = inner_form(h, o, want_learned);
   const bool persist = form != InnerForm::kGraph;
-  const bool pending = form == InnerForm::kFused;
+  const bool pending =
+      form == InnerForm::kFused ||
+      (form == InnerForm::kSplit &&
+       persist_defers_d(want_learned,
+                        h->N >= kPersistPrefetchMinRows ? kPersistPrefetchRows : 0));
   // PERSISTENT on a matrix without the band form runs as GRAPH.
   const bool graph_loop =
       (o.loop == CGX_LOOP_GRAPH || o.loop == CGX_LOOP_PERSISTENT ||
@@ -2135,7 +2140,7 @@ static cgx_status solve_mixed(cgx_handle *h, const cgx_options &o,
   auto jacobi_start = [&] {
     k_inner_start<<<grid_stream(h, h->N), kThreads, 0, h->stream>>>(
         h->N, h->r64, h->r32, h->d32, h->p32, h->C32, h->st, h->partials,
-        ticket(h, kTicketInnerStart), pending ? h->z32 : nullptr);
+        ticket(h, kTicketInnerStart), form == InnerForm::kFused ? h->z32 : nullptr);
     return cudaGetLastError();
   };
   GraphEntry *gj = nullptr, *gl = nullptr;

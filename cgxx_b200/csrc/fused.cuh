@@ -291,11 +291,10 @@ __device__ __forceinline__ void gband_t_rows(const GBandView &B, const float *r,
   }
 }
 
-// r -= a q (k_inner_update_z / k_inner_update) and d += a p (the d half of
-// k_inner_direction_z / k_inner_direction; p does not change before the
-// direction phase); this thread's partial of <r,r> and, with C (Jacobi), of
-// <r,Cr>.
-template <int TPB>
+// r -= a q (k_inner_update_z / k_inner_update), and with D also d += a p
+// (the d half of k_inner_direction; p does not change before the direction
+// phase); this thread's partial of <r,r> and, with C (Jacobi), of <r,Cr>.
+template <int TPB, bool D>
 __device__ __forceinline__ void update_rows(int N, float *r, const float *q, float *d,
                                             const float *p, const float *C, float a,
                                             double &rr, double &rz) {
@@ -309,8 +308,16 @@ __device__ __forceinline__ void update_rows(int N, float *r, const float *q, flo
   rows4<TPB>(
       N,
       [&](int i) {
-        float4 rv = ldv4(r, i), dv = ldv4(d, i);
-        const float4 qv = ldv4(q, i), pv = ldv4(p, i);
+        // Every load before the first store: the compiler cannot tell that
+        // r, d and p do not overlap, so a load after a store would wait
+        // for it.
+        float4 rv = ldv4(r, i), dv = make_float4(0.f, 0.f, 0.f, 0.f);
+        const float4 qv = ldv4(q, i);
+        float4 pv = dv;
+        if (D) {
+          dv = ldv4(d, i);
+          pv = ldv4(p, i);
+        }
         rv.x = fmaf(na, qv.x, rv.x);
         rv.y = fmaf(na, qv.y, rv.y);
         rv.z = fmaf(na, qv.z, rv.z);
@@ -320,7 +327,7 @@ __device__ __forceinline__ void update_rows(int N, float *r, const float *q, flo
         dv.z = fmaf(a, pv.z, dv.z);
         dv.w = fmaf(a, pv.w, dv.w);
         reinterpret_cast<float4 *>(r)[i] = rv;
-        reinterpret_cast<float4 *>(d)[i] = dv;
+        if (D) reinterpret_cast<float4 *>(d)[i] = dv;
         const float4 cv =
             C ? __ldg(reinterpret_cast<const float4 *>(C) + i) : make_float4(0.f, 0.f, 0.f, 0.f);
         dots(rv.x, cv.x);
@@ -331,20 +338,23 @@ __device__ __forceinline__ void update_rows(int N, float *r, const float *q, flo
       [&](int i) {
         const float ri = fmaf(na, ldv(q + i), ldv(r + i));
         r[i] = ri;
-        d[i] = fmaf(a, ldv(p + i), ldv(d + i));
+        if (D) d[i] = fmaf(a, ldv(p + i), ldv(d + i));
         dots(ri, C ? __ldg(C + i) : 0.f);
       });
 }
 
 // p = z + b p (learned, k_inner_direction_z) or p = C r + b p (Jacobi,
-// k_inner_direction: z = nullptr).
-template <int TPB>
-__device__ __forceinline__ void direction_rows(int N, float *p, const float *z,
-                                               const float *r, const float *C, float b) {
+// k_inner_direction: z = nullptr); with D first d += a p, p read once for
+// both updates.
+template <int TPB, bool D>
+__device__ __forceinline__ void direction_rows(int N, float *p, float *d, const float *z,
+                                               const float *r, const float *C, float a,
+                                               float b) {
   rows4<TPB>(
       N,
       [&](int i) {
         const float4 pv = ldv4(p, i);
+        float4 dv = D ? ldv4(d, i) : make_float4(0.f, 0.f, 0.f, 0.f);
         float4 zv;
         if (z) {
           zv = ldv4(z, i);
@@ -352,13 +362,22 @@ __device__ __forceinline__ void direction_rows(int N, float *p, const float *z,
           const float4 rv = ldv4(r, i), cv = __ldg(reinterpret_cast<const float4 *>(C) + i);
           zv = make_float4(cv.x * rv.x, cv.y * rv.y, cv.z * rv.z, cv.w * rv.w);
         }
+        if (D) {
+          dv.x = fmaf(a, pv.x, dv.x);
+          dv.y = fmaf(a, pv.y, dv.y);
+          dv.z = fmaf(a, pv.z, dv.z);
+          dv.w = fmaf(a, pv.w, dv.w);
+          reinterpret_cast<float4 *>(d)[i] = dv;
+        }
         reinterpret_cast<float4 *>(p)[i] =
             make_float4(fmaf(b, pv.x, zv.x), fmaf(b, pv.y, zv.y), fmaf(b, pv.z, zv.z),
                         fmaf(b, pv.w, zv.w));
       },
       [&](int i) {
+        const float pi = ldv(p + i);
         const float zi = z ? ldv(z + i) : __ldg(C + i) * ldv(r + i);
-        p[i] = fmaf(b, ldv(p + i), zi);
+        if (D) d[i] = fmaf(a, pi, ldv(d + i));
+        p[i] = fmaf(b, pi, zi);
       });
 }
 

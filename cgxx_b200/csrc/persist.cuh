@@ -255,22 +255,35 @@ __global__ void __launch_bounds__(TPB, MINB)
   persist_publish(st, alpha, beta, rho, res, it, total, par, ok);
 }
 
+// Where the split form applies d += a p. Deferred: in the direction phase,
+// which reads p once for both updates (as k_inner_direction does), the
+// loop's last update left pending (k_outer_update_pending applies it with
+// p[0] and the published a); 4 bytes fewer per row and iteration. Else in
+// the residual phase, d complete when the loop stops. Measured (same box):
+// deferred, 160^3 learned 22.8 against 23.5 ms; 128^3 learned 10.72 against
+// 10.62 ms, and the Jacobi and SELL-U forms 1-1.5 % slower. So only the
+// learned form with the L2 prefetch (the largest grids) defers.
+__host__ __device__ constexpr bool persist_defers_d(bool learned, int pf) {
+  return learned && pf > 0;
+}
+
 // The split form: the graph iteration's kernels as phases (fused.cuh), five
 // barriers per learned iteration and three per Jacobi one, no values formed
-// twice and no ping-pong buffers (p[0], r[0] only). d is complete when the
-// loop stops (the plain k_outer_update applies it).
+// twice and no ping-pong buffers (p[0], r[0] only). [d += a p] is in phase B
+// or, deferred (persist_defers_d), in phase E.
 //
 //   learned: A  q = A p                                   | <p,q> -> a
-//            B  r -= a q, d += a p                        | <r,r> -> test
+//            B  r -= a q [, d += a p]                     | <r,r> -> test
 //            C  y = G^T r                                 |
 //            D  z = G y + eps C r                         | <r,z> -> b
-//            E  p = z + b p                               |
+//            E  [d += a p,] p = z + b p                   |
 //   Jacobi:  A  as above                                  | <p,q> -> a
 //            B  r -= a q, d += a p                        | <r,r>, <r,Cr> -> test, b
 //            E  p = C r + b p                             |
 template <bool LEARNED, int TPB, int MINB, int PF>
 __global__ void __launch_bounds__(TPB, MINB)
     k_inner_persist_split(BandView<4> A, GBandView G, PersistArgs a, CgState *st) {
+  constexpr bool DEFER = persist_defers_d(LEARNED, PF);
   double rho = st->in_rho, alpha = 0.0, beta = 0.0, res = 0.0;
   const double nrm0 = st->in_nrm0, tol = st->in_tol;
   int total = st->total_inner;
@@ -287,7 +300,8 @@ __global__ void __launch_bounds__(TPB, MINB)
     alpha = rho / sum_partials<TPB>(slot0);
     {
       double rr, rz;
-      update_rows<TPB>(N, r, a.q, a.d, p, LEARNED ? nullptr : a.C, (float)alpha, rr, rz);
+      update_rows<TPB, !DEFER>(N, r, a.q, a.d, p, LEARNED ? nullptr : a.C, (float)alpha,
+                               rr, rz);
       put_partial<TPB>(rr, slot1);
       if (!LEARNED) put_partial<TPB>(rz, slot2);
     }
@@ -308,7 +322,8 @@ __global__ void __launch_bounds__(TPB, MINB)
     const double rzn = sum_partials<TPB>(slot2);
     beta = rzn / rho;
     rho = rzn;
-    direction_rows<TPB>(N, p, LEARNED ? a.z : nullptr, r, a.C, (float)beta);
+    direction_rows<TPB, DEFER>(N, p, a.d, LEARNED ? a.z : nullptr, r, a.C, (float)alpha,
+                               (float)beta);
     if (!(ok = grid_sync(a.sync, ++bar * nb))) break;
   }
   persist_publish(st, alpha, beta, rho, res, it, total, 0, ok);
@@ -388,7 +403,8 @@ __global__ void __launch_bounds__(TPB, MINB)
     alpha = rho / sum_partials<TPB>(slot0);
     {
       double rr, rz;
-      update_rows<TPB>(N, r, a.q, a.d, p, LEARNED ? nullptr : a.C, (float)alpha, rr, rz);
+      update_rows<TPB, true>(N, r, a.q, a.d, p, LEARNED ? nullptr : a.C, (float)alpha, rr,
+                             rz);
       put_partial<TPB>(rr, slot1);
       if (!LEARNED) put_partial<TPB>(rz, slot2);
     }
@@ -412,7 +428,8 @@ __global__ void __launch_bounds__(TPB, MINB)
     const double rzn = sum_partials<TPB>(slot2);
     beta = rzn / rho;
     rho = rzn;
-    direction_rows<TPB>(N, p, LEARNED ? a.z : nullptr, r, a.C, (float)beta);
+    direction_rows<TPB, false>(N, p, a.d, LEARNED ? a.z : nullptr, r, a.C, (float)alpha,
+                               (float)beta);
     if (!(ok = grid_sync(a.sync, ++bar * nb))) break;
   }
   persist_publish(st, alpha, beta, rho, res, it, total, 0, ok);

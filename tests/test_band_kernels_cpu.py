@@ -273,13 +273,16 @@ def test_persistent_iteration_matches_pcg(case, learned):
     assert np.allclose(xf, xr, rtol=2e-3, atol=2e-3 * np.abs(xr).max())
 
 
+@pytest.mark.parametrize("defer", [False, True])
 @pytest.mark.parametrize("learned", [True, False])
 @pytest.mark.parametrize("case", ["grid3d", "odd"])
-def test_split_iteration_matches_pcg(case, learned):
-    """k_inner_persist_split's phases in its order (q = A p | r -= a q,
-    d += a p | y = G^T r | z = G y + eps C r | p = z + b p, Jacobi without
-    the two factor phases and with p = C r + b p) against a plain PCG; d is
-    complete when the loop stops."""
+def test_split_iteration_matches_pcg(case, learned, defer):
+    """k_inner_persist_split's phases in its order (q = A p | r -= a q
+    [, d += a p] | y = G^T r | z = G y + eps C r | [d += a p,] p = z + b p;
+    Jacobi without the two factor phases and with p = C r + b p) against a
+    plain PCG. The loop stops after its residual phase; with the d update
+    deferred to the direction phase, the last one is pending and applied at
+    the end, as k_outer_update_pending does."""
     A, U, Gb, d4 = _setup(case)
     N = A.N
     Gl, Gt = lower_csr(Gb, d4)
@@ -302,11 +305,14 @@ def test_split_iteration_matches_pcg(case, learned):
     d = np.zeros(N, np.float32)
     rho = float(r.astype(np.float64) @ z)
     zero = Buf(np.zeros(N))
-    for _ in range(iters):
+    for k in range(iters):
         _, _, q = band_dir(d4, Ub, zero, Buf(p), zero, 0.0, 1.0, N)  # q = A p
         al = rho / float(p.astype(np.float64) @ q)
         r = fma(-al, q, r)
-        d = fma(al, p, d)
+        if not defer:
+            d = fma(al, p, d)
+        if k == iters - 1:
+            break  # the residual test stops the loop here
         if learned:
             _, y = gband_res(d4, Gbb, Buf(r), zero, 0.0, N)  # y = G^T r
             z = gband_z(d4, Gbb, Buf(y), Buf(r), C, eps, N)
@@ -314,8 +320,11 @@ def test_split_iteration_matches_pcg(case, learned):
             z = (Cv * r).astype(np.float32)
         rn = float(r.astype(np.float64) @ z)
         be, rho = rn / rho, rn
+        if defer:
+            d = fma(al, p, d)
         p = fma(be, p, z)
-    assert np.allclose(d, xr, rtol=2e-3, atol=2e-3 * np.abs(xr).max())
+    xf = fma(al, p, d) if defer else d  # the pending update
+    assert np.allclose(xf, xr, rtol=2e-3, atol=2e-3 * np.abs(xr).max())
 
 
 @pytest.mark.parametrize("split", [False, True])

@@ -21,6 +21,14 @@ PHASES = {
         ("z = G y + eps C r", ["Gb8", "y", "r", "C"], ["z"]),
         ("p = z + b p", ["p", "z"], ["p"]),
     ],
+    # N >= 3M rows: d += a p moves into the direction phase (p read once)
+    ("split-deferred", True): [
+        ("q = A p", ["U16", "p"], ["q"]),
+        ("r -= a q", ["r", "q"], ["r"]),
+        ("y = G^T r", ["Gb8", "r"], ["y"]),
+        ("z = G y + eps C r", ["Gb8", "y", "r", "C"], ["z"]),
+        ("d += a p, p = z + b p", ["p", "z", "d"], ["p", "d"]),
+    ],
     ("split", False): [
         ("q = A p", ["U16", "p"], ["q"]),
         ("r -= a q, d += a p, <r,Cr>", ["r", "q", "d", "p", "C"], ["r", "d"]),
@@ -57,13 +65,20 @@ def test_persist_bytes_restate_the_phases(form, code, learned):
     assert last == _bytes(phases[:2])
 
 
+def test_deferred_split_bytes_restate_the_phases():
+    phases = PHASES[("split-deferred", True)]
+    full, last = bench.PERSIST_BYTES_DEFERRED[(2, True)]
+    assert full == _bytes(phases)
+    assert last == _bytes(phases[:2])
+
+
 def test_persist_roofline_divides_the_iterations_bytes_by_the_launch_time():
     args = types.SimpleNamespace(path="learned", graph=0, n=160, stencil=7)
     N = 4_096_000
     results = [{"inner_form": 2, "fell_back": 0, "inner_launches": 3, "iterations": 330,
                 "inner_ms": 24.0} for _ in range(2)]
     roof = bench.persist_roofline(args, results, N, 6530.0, "measured")
-    full, last = bench.PERSIST_BYTES[(2, True)]
+    full, last = bench.PERSIST_BYTES_DEFERRED[(2, True)]  # N >= 3M rows
     per_solve = (330 * full - 3 * (full - last)) * N
     assert roof["algorithmic_bytes"] == pytest.approx(per_solve / 3)
     assert roof["launch_us"] == pytest.approx(8000.0)
@@ -82,3 +97,13 @@ def test_persist_roofline_skips_other_forms():
     args.path = "plain"
     r[0]["inner_form"] = 2
     assert bench.persist_roofline(args, r, 2_097_152, 6530.0, "measured") is None
+
+
+def test_persist_roofline_takes_the_undeferred_bytes_below_3m_rows():
+    args = types.SimpleNamespace(path="learned", graph=0, n=128, stencil=7)
+    N = 2_097_152
+    r = [{"inner_form": 2, "fell_back": 0, "inner_launches": 2, "iterations": 254,
+          "inner_ms": 10.0}]
+    roof = bench.persist_roofline(args, r, N, 6530.0, "measured")
+    full, last = bench.PERSIST_BYTES[(2, True)]
+    assert roof["algorithmic_bytes"] == pytest.approx((254 * full - 2 * (full - last)) * N / 2)
