@@ -260,9 +260,10 @@ __global__ void __launch_bounds__(TPB, MINB)
 // loop's last update left pending (k_outer_update_pending applies it with
 // p[0] and the published a); 4 bytes fewer per row and iteration. Else in
 // the residual phase, d complete when the loop stops. Measured (same box):
-// deferred, 160^3 learned 22.8 against 23.5 ms; 128^3 learned 10.72 against
-// 10.62 ms, and the Jacobi and SELL-U forms 1-1.5 % slower. So only the
-// learned form with the L2 prefetch (the largest grids) defers.
+// deferred, 160^3 learned 22.93 against 23.66 ms; deferring everywhere made
+// 128^3 learned 10.72 against 10.62 ms and the Jacobi and SELL-U forms
+// 1-1.5 % slower. So only the learned form with the L2 prefetch (the
+// largest grids) defers.
 __host__ __device__ constexpr bool persist_defers_d(bool learned, int pf) {
   return learned && pf > 0;
 }
